@@ -1,0 +1,363 @@
+// api.cpp — the C ABI (include/beep.h) over the device graph build and the
+// counting kernels.
+#include <algorithm>
+#include <cstdio>
+
+#include "internal.h"
+
+namespace beep {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+beep_status fail(beep_status s, const std::string &msg) {
+    set_error(msg);
+    return s;
+}
+
+namespace {
+
+beep_status bind(beep_ctx *ctx) {
+    if (!ctx)
+        return fail(BEEP_ERR_INVALID_ARG, "null context");
+    BEEP_CUDA_TRY(cudaSetDevice(ctx->impl.device));
+    return BEEP_OK;
+}
+
+// Copy a host array to a device buffer through the context's stream.
+template <typename T> beep_status upload(Ctx *ctx, DevBuf &dst, const T *src, size_t count) {
+    BEEP_TRY(dst.reserve(std::max<size_t>(count, 1) * sizeof(T)));
+    if (count)
+        BEEP_CUDA_TRY(cudaMemcpyAsync(dst.ptr, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    return BEEP_OK;
+}
+
+} // namespace
+} // namespace beep
+
+using namespace beep;
+
+extern "C" {
+
+size_t beep_last_error(char *buf, size_t len) {
+    const std::string &e = g_last_error;
+    if (buf && len) {
+        size_t n = std::min(len - 1, e.size());
+        std::memcpy(buf, e.data(), n);
+        buf[n] = '\0';
+    }
+    return e.size();
+}
+
+const char *beep_status_string(beep_status s) {
+    switch (s) {
+    case BEEP_OK:
+        return "ok";
+    case BEEP_ERR_INVALID_ARG:
+        return "invalid argument";
+    case BEEP_ERR_IO:
+        return "i/o error";
+    case BEEP_ERR_PARSE:
+        return "parse error";
+    case BEEP_ERR_UNSUPPORTED:
+        return "unsupported";
+    case BEEP_ERR_CUDA:
+        return "cuda error";
+    case BEEP_ERR_OUT_OF_MEMORY:
+        return "out of memory";
+    case BEEP_ERR_TIMEOUT:
+        return "timeout";
+    case BEEP_ERR_INTERNAL:
+        return "internal error";
+    }
+    return "unknown";
+}
+
+beep_status beep_ctx_create(int device, void *stream, beep_ctx **out) {
+    if (!out)
+        return fail(BEEP_ERR_INVALID_ARG, "null output");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(BEEP_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= ndev)
+        return fail(BEEP_ERR_INVALID_ARG, "device id out of range");
+    auto *c = new beep_ctx;
+    c->impl.device = device;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&c->impl.num_sms, cudaDevAttrMultiProcessorCount, device);
+    int optin = 0;
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    c->impl.smem_optin = (size_t)optin;
+    if (e == cudaSuccess) {
+        if (stream) {
+            c->impl.stream = static_cast<cudaStream_t>(stream);
+        } else {
+            e = cudaStreamCreateWithFlags(&c->impl.stream, cudaStreamNonBlocking);
+            c->impl.own_stream = true;
+        }
+    }
+    if (e == cudaSuccess)
+        e = cudaMallocHost(&c->impl.h_pinned, 64);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(BEEP_ERR_CUDA, std::string("context setup: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return BEEP_OK;
+}
+
+beep_status beep_ctx_destroy(beep_ctx *ctx) {
+    if (!ctx)
+        return BEEP_OK;
+    cudaSetDevice(ctx->impl.device);
+    cudaStreamSynchronize(ctx->impl.stream);
+    ctx->impl.scratch.release();
+    ctx->impl.scratch2.release();
+    ctx->impl.arena.release();
+    ctx->impl.counter.release();
+    if (ctx->impl.h_pinned)
+        cudaFreeHost(ctx->impl.h_pinned);
+    if (ctx->impl.own_stream)
+        cudaStreamDestroy(ctx->impl.stream);
+    delete ctx;
+    return BEEP_OK;
+}
+
+beep_status beep_ctx_set_wait_timeout(beep_ctx *ctx, double ms) {
+    if (!ctx || !(ms > 0))
+        return fail(BEEP_ERR_INVALID_ARG, "bad timeout");
+    ctx->impl.wait_timeout_ms = ms;
+    return BEEP_OK;
+}
+
+beep_status beep_ctx_kernel_launches(const beep_ctx *ctx, uint64_t *out) {
+    if (!ctx || !out)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_ctx_kernel_launches: bad arguments");
+    *out = ctx->impl.launches;
+    return BEEP_OK;
+}
+
+beep_status beep_graph_from_device_csr(beep_ctx *ctx, int64_t n, int64_t m, const int32_t *d_row_ptr,
+                                       const int32_t *d_col_ind, beep_graph **out) {
+    if (!out || !d_row_ptr || (m > 0 && !d_col_ind) || n < 0 || m < 0)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_graph_from_device_csr: bad arguments");
+    *out = nullptr;
+    BEEP_TRY(bind(ctx));
+    auto *g = new beep_graph;
+    g->ctx = ctx;
+    g->impl.device = ctx->impl.device;
+    beep_status s = graph_build_from_device_csr(&ctx->impl, &g->impl, n, m,
+                                                reinterpret_cast<const uint32_t *>(d_row_ptr),
+                                                reinterpret_cast<const uint32_t *>(d_col_ind));
+    if (s != BEEP_OK) {
+        delete g;
+        return s;
+    }
+    *out = g;
+    return BEEP_OK;
+}
+
+beep_status beep_graph_from_csr(beep_ctx *ctx, int64_t n, int64_t m, const int32_t *row_ptr, const int32_t *col_ind,
+                                beep_graph **out) {
+    if (!out || !row_ptr || (m > 0 && !col_ind) || n < 0 || m < 0)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_graph_from_csr: bad arguments");
+    *out = nullptr;
+    if (row_ptr[0] != 0 || row_ptr[n] != m)
+        return fail(BEEP_ERR_INVALID_ARG, "row_ptr must start at 0 and end at m");
+    BEEP_TRY(bind(ctx));
+    auto *g = new beep_graph;
+    g->ctx = ctx;
+    g->impl.device = ctx->impl.device;
+    // Upload straight into the graph's buffers; the build keeps them when the
+    // rows are already sorted and simple.
+    beep_status s = upload(&ctx->impl, g->impl.row_ptr, reinterpret_cast<const uint32_t *>(row_ptr), (size_t)n + 1);
+    if (s == BEEP_OK)
+        s = upload(&ctx->impl, g->impl.col, reinterpret_cast<const uint32_t *>(col_ind), (size_t)m);
+    if (s == BEEP_OK)
+        s = graph_build_from_device_csr(&ctx->impl, &g->impl, n, m, g->impl.row_ptr.as<uint32_t>(),
+                                        g->impl.col.as<uint32_t>());
+    if (s != BEEP_OK) {
+        delete g;
+        return s;
+    }
+    *out = g;
+    return BEEP_OK;
+}
+
+beep_status beep_graph_from_edges(beep_ctx *ctx, int64_t n_edges, const uint32_t *src, const uint32_t *dst,
+                                  beep_graph **out) {
+    if (!out || n_edges < 0 || (n_edges > 0 && (!src || !dst)))
+        return fail(BEEP_ERR_INVALID_ARG, "beep_graph_from_edges: bad arguments");
+    *out = nullptr;
+    BEEP_TRY(bind(ctx));
+    DevBuf ds, dd;
+    BEEP_TRY(upload(&ctx->impl, ds, src, (size_t)n_edges));
+    BEEP_TRY(upload(&ctx->impl, dd, dst, (size_t)n_edges));
+    auto *g = new beep_graph;
+    g->ctx = ctx;
+    g->impl.device = ctx->impl.device;
+    beep_status s = graph_build_from_device_edges(&ctx->impl, &g->impl, n_edges, ds.as<uint32_t>(), dd.as<uint32_t>());
+    cudaStreamSynchronize(ctx->impl.stream);
+    if (s != BEEP_OK) {
+        delete g;
+        return s;
+    }
+    *out = g;
+    return BEEP_OK;
+}
+
+beep_status beep_graph_load_bel(beep_ctx *ctx, const char *path, beep_graph **out) {
+    if (!path || !out)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_graph_load_bel: bad arguments");
+    std::vector<uint32_t> src, dst;
+    BEEP_TRY(read_bel(path, src, dst));
+    return beep_graph_from_edges(ctx, (int64_t)src.size(), src.data(), dst.data(), out);
+}
+
+beep_status beep_graph_info_get(const beep_graph *g, beep_graph_info *out) {
+    if (!g || !out)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_graph_info_get: bad arguments");
+    std::memset(out, 0, sizeof(*out));
+    out->n = g->impl.n;
+    out->m = g->impl.m;
+    out->max_degree = g->impl.max_degree;
+    out->cutoff = g->impl.cutoff;
+    return BEEP_OK;
+}
+
+beep_status beep_graph_csr(const beep_graph *g, int32_t *row_ptr, int32_t *col_ind) {
+    if (!g || !row_ptr || (g->impl.m > 0 && !col_ind))
+        return fail(BEEP_ERR_INVALID_ARG, "beep_graph_csr: bad arguments");
+    BEEP_TRY(bind(g->ctx));
+    cudaStream_t s = g->ctx->impl.stream;
+    BEEP_CUDA_TRY(cudaMemcpyAsync(row_ptr, g->impl.row_ptr.ptr, (size_t)(g->impl.n + 1) * 4, cudaMemcpyDeviceToHost, s));
+    if (g->impl.m > 0)
+        BEEP_CUDA_TRY(cudaMemcpyAsync(col_ind, g->impl.col.ptr, (size_t)g->impl.m * 4, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    return BEEP_OK;
+}
+
+beep_status beep_graph_destroy(beep_graph *g) {
+    if (!g)
+        return BEEP_OK;
+    if (g->ctx) {
+        cudaSetDevice(g->impl.device);
+        cudaStreamSynchronize(g->ctx->impl.stream);
+    }
+    delete g;
+    return BEEP_OK;
+}
+
+beep_status beep_query_load_mtx(const char *path, beep_query **out) {
+    if (!path || !out)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_query_load_mtx: bad arguments");
+    *out = nullptr;
+    std::vector<int32_t> src, dst;
+    BEEP_TRY(read_mtx(path, src, dst));
+    auto *q = new beep_query;
+    beep_status s = query_from_edges(src, dst, &q->impl);
+    if (s != BEEP_OK) {
+        delete q;
+        return s;
+    }
+    *out = q;
+    return BEEP_OK;
+}
+
+beep_status beep_query_from_edges(int32_t n_edges, const int32_t *src, const int32_t *dst, beep_query **out) {
+    if (!out || n_edges <= 0 || !src || !dst)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_query_from_edges: bad arguments");
+    *out = nullptr;
+    std::vector<int32_t> s(src, src + n_edges), d(dst, dst + n_edges);
+    auto *q = new beep_query;
+    beep_status st = query_from_edges(s, d, &q->impl);
+    if (st != BEEP_OK) {
+        delete q;
+        return st;
+    }
+    *out = q;
+    return BEEP_OK;
+}
+
+beep_status beep_query_destroy(beep_query *q) {
+    delete q;
+    return BEEP_OK;
+}
+
+beep_status beep_query_plan(const beep_query *q, beep_mode mode, beep_plan_info *out) {
+    if (!q || !out)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_query_plan: bad arguments");
+    if (mode != BEEP_MODE_SGM && mode != BEEP_MODE_SGC)
+        return fail(BEEP_ERR_INVALID_ARG, "unknown mode");
+    QueryPlan p;
+    BEEP_TRY(compile_plan(q->impl.qn, q->impl.row_ptr, q->impl.col, mode, &p));
+    *out = p.info;
+    return BEEP_OK;
+}
+
+beep_status beep_count_ex(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t options,
+                          beep_stats *stats) {
+    if (!g || !q)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_count: null graph or query");
+    if (mode != BEEP_MODE_SGM && mode != BEEP_MODE_SGC)
+        return fail(BEEP_ERR_INVALID_ARG, "unknown mode");
+    if (ctx && g->ctx && ctx->impl.device != g->impl.device)
+        return fail(BEEP_ERR_INVALID_ARG, "graph lives on another device");
+    if (!ctx)
+        ctx = g->ctx;
+    BEEP_TRY(bind(ctx));
+    QueryPlan p;
+    BEEP_TRY(compile_plan(q->impl.qn, q->impl.row_ptr, q->impl.col, mode, &p));
+    beep_stats st;
+    BEEP_TRY(run_count(&ctx->impl, &g->impl, p, options, nullptr, &st));
+    ctx->impl.launches += (uint64_t)st.kernel_launches;
+    if (stats)
+        *stats = st;
+    return BEEP_OK;
+}
+
+beep_status beep_count(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_mode mode, uint64_t *out_count) {
+    if (!out_count)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_count: null output");
+    beep_stats st;
+    BEEP_TRY(beep_count_ex(ctx, g, q, mode, 0, &st));
+    *out_count = st.count;
+    return BEEP_OK;
+}
+
+beep_status beep_enumerate(beep_ctx *ctx, beep_graph *g, const beep_query *q, uint64_t k, int32_t *out_tuples,
+                           uint64_t *n_out, uint64_t *total_count) {
+    if (!g || !q || !n_out || (k > 0 && !out_tuples))
+        return fail(BEEP_ERR_INVALID_ARG, "beep_enumerate: bad arguments");
+    if (!ctx)
+        ctx = g->ctx;
+    BEEP_TRY(bind(ctx));
+    QueryPlan p;
+    BEEP_TRY(compile_plan(q->impl.qn, q->impl.row_ptr, q->impl.col, BEEP_MODE_SGM, &p));
+    const size_t K = (size_t)p.info.K;
+    DevBuf dout;
+    BEEP_TRY(dout.reserve(std::max<uint64_t>(k, 1) * K * 4));
+    EnumRequest er;
+    er.k = k;
+    er.d_out = dout.as<int32_t>();
+    beep_stats st;
+    BEEP_TRY(run_count(&ctx->impl, &g->impl, p, 0, k > 0 ? &er : nullptr, &st));
+    ctx->impl.launches += (uint64_t)st.kernel_launches;
+    const uint64_t got = std::min<uint64_t>(k, st.count);
+    if (got)
+        BEEP_CUDA_TRY(cudaMemcpyAsync(out_tuples, dout.ptr, got * K * 4, cudaMemcpyDeviceToHost, ctx->impl.stream));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(ctx->impl.stream));
+    *n_out = got;
+    if (total_count)
+        *total_count = st.count;
+    return BEEP_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,559 @@
+// graph.cu — on-device CSR build, dedup, iterated peeling and priority
+// relabelling.
+//
+// The reference builds the CSR on the host (include/CSRCOO.cuh:37-80), peels
+// with many synchronous launches and managed-memory reads
+// (subgraph_matching.cuh:685-764) and orders every adjacency list with two
+// global thrust::stable_sort passes over a triplet array
+// (subgraph_matching.cuh:1282-1336). Here the whole graph is relabelled once
+// per (peel threshold, order) by the same priority, so every sorted row of the
+// relabelled CSR is the reference's oriented row and the split point is a
+// lower_bound.
+#include <cmath>
+
+#include <cub/cub.cuh>
+
+#include "internal.h"
+
+namespace beep {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__global__ void k_check_csr(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n, int64_t m,
+                            unsigned *bad) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+        const uint32_t b = rp[v], e = rp[v + 1];
+        if (e < b || e > m) {
+            if (lane == 0)
+                atomicOr(bad, 1u);
+            continue;
+        }
+        for (uint32_t i = b + lane; i < e; i += 32) {
+            const uint32_t w = col[i];
+            bool ok = w < n && w != (uint32_t)v && (i == b || col[i - 1] < w);
+            if (!ok)
+                atomicOr(bad, 1u);
+        }
+    }
+}
+
+__global__ void k_csr_keys(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n,
+                           uint64_t *keys) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+        const uint32_t b = rp[v], e = rp[v + 1];
+        for (uint32_t i = b + lane; i < e; i += 32) {
+            const uint32_t w = col[i];
+            keys[i] = (w == (uint32_t)v) ? ~0ull : (((uint64_t)v << 32) | w);
+        }
+    }
+}
+
+__global__ void k_edge_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst, int64_t ne,
+                            uint64_t *keys, unsigned *max_id) {
+    uint32_t mx = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = src[i], d = dst[i];
+        keys[i] = (s == d) ? ~0ull : (((uint64_t)s << 32) | d);
+        mx = max(mx, max(s, d));
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+    if ((threadIdx.x & 31) == 0)
+        atomicMax(max_id, mx);
+}
+
+// Keys are sorted and unique; the self-loop sentinel (~0) sorts last.
+__global__ void k_keys_to_coo(const uint64_t *__restrict__ keys, int64_t m, uint32_t *col, uint32_t *deg) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = keys[i];
+        col[i] = (uint32_t)k;
+        atomicAdd(&deg[k >> 32], 1u);
+    }
+}
+
+__global__ void k_degree_stats(const uint32_t *__restrict__ rp, int64_t n, unsigned long long *sumsq,
+                               unsigned *maxdeg) {
+    unsigned long long s = 0;
+    uint32_t mx = 0;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t d = rp[v + 1] - rp[v];
+        s += (unsigned long long)d * d;
+        mx = max(mx, d);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(kFull, s, o);
+        mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(sumsq, s);
+        atomicMax(maxdeg, mx);
+    }
+}
+
+// ---- peeling --------------------------------------------------------------
+
+__global__ void k_peel_init(const uint32_t *__restrict__ rp, int64_t n, uint32_t *deg, uint8_t *alive) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        deg[v] = rp[v + 1] - rp[v];
+        alive[v] = 1;
+    }
+}
+
+// Vertices with degree in [1, min_qdeg) are removed together
+// (bucket_scan window, subgraph_matching.cuh:66-109, 703).
+__global__ void k_peel_mark(const uint32_t *__restrict__ deg, uint8_t *alive, int64_t n, uint32_t min_qdeg,
+                            unsigned long long *removed) {
+    unsigned long long c = 0;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t d = deg[v];
+        if (d >= 1 && d < min_qdeg) {
+            alive[v] = 0;
+            ++c;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        c += __shfl_xor_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0 && c)
+        atomicAdd(removed, c);
+}
+
+// Degree after dropping every edge with a removed endpoint
+// (remove_edges_connected_to_node + warp_detect_deleted_edges,
+// common_utils.cuh:99-133, 217-246).
+__global__ void k_peel_degree(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
+                              const uint8_t *__restrict__ alive, int64_t n, uint32_t *deg) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+        if (!alive[v]) {
+            if (lane == 0)
+                deg[v] = 0;
+            continue;
+        }
+        const uint32_t b = rp[v], e = rp[v + 1];
+        uint32_t c = 0;
+        for (uint32_t i = b + lane; i < e; i += 32)
+            c += alive[col[i]];
+        c = __reduce_add_sync(kFull, c);
+        if (lane == 0)
+            deg[v] = c;
+    }
+}
+
+// ---- relabelling -----------------------------------------------------------
+
+// Priority key (subgraph_matching.cuh:1299-1331, host_utils.cuh:230-246):
+// ascending (degree, id) or descending degree with ties by ascending id.
+// Vertices left with no edge get the largest key and are dropped.
+__global__ void k_prio_keys(const uint32_t *__restrict__ deg, int64_t n, uint32_t maxdeg, int asc,
+                            uint64_t *keys, unsigned long long *n_alive) {
+    unsigned long long c = 0;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t d = deg[v];
+        uint64_t hi;
+        if (d == 0) {
+            hi = maxdeg;
+        } else {
+            hi = asc ? (uint64_t)(d - 1) : (uint64_t)(maxdeg - d);
+            ++c;
+        }
+        keys[v] = (hi << 32) | (uint64_t)v;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        c += __shfl_xor_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0 && c)
+        atomicAdd(n_alive, c);
+}
+
+__global__ void k_rank(const uint64_t *__restrict__ keys, int64_t n_alive, uint32_t *orig, uint32_t *rank,
+                       const uint32_t *__restrict__ deg, uint32_t *new_deg) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_alive;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = (uint32_t)keys[i];
+        orig[i] = v;
+        rank[v] = (uint32_t)i;
+        new_deg[i] = deg[v];
+    }
+}
+
+// Row i of the relabelled graph: ranks of the surviving neighbours of
+// orig[i], compacted in input order (sorted afterwards).
+__global__ void k_fill_rows(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
+                            const uint32_t *__restrict__ orig, const uint32_t *__restrict__ rank,
+                            const uint32_t *__restrict__ new_rp, int64_t n_alive, uint32_t *new_col) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_alive; i += warps) {
+        const uint32_t v = orig[i];
+        const uint32_t b = rp[v], e = rp[v + 1];
+        uint32_t out = new_rp[i];
+        for (uint32_t base = b; base < e; base += 32) {
+            const uint32_t idx = base + lane;
+            uint32_t r = 0xffffffffu;
+            if (idx < e)
+                r = rank[col[idx]];
+            const bool keep = r != 0xffffffffu;
+            const unsigned bal = __ballot_sync(kFull, keep);
+            if (keep)
+                new_col[out + __popc(bal & ((1u << lane) - 1u))] = r;
+            out += __popc(bal);
+        }
+    }
+}
+
+// split[i] = number of neighbours with a smaller new id (lower_bound of i).
+__global__ void k_split(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n,
+                        uint32_t *split) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = rp[i], hi = rp[i + 1];
+        const uint32_t b = lo;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (col[mid] < (uint32_t)i)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        split[i] = lo - b;
+    }
+}
+
+inline int grid_for(int64_t items, int block, int num_sms) {
+    int64_t g = (items + block - 1) / block;
+    int64_t cap = (int64_t)num_sms * 32;
+    if (g > cap)
+        g = cap;
+    if (g < 1)
+        g = 1;
+    return (int)g;
+}
+
+// Bump allocator over a grow-only buffer.
+struct Carve {
+    char *base;
+    size_t off = 0;
+    explicit Carve(void *b) : base(static_cast<char *>(b)) {}
+    template <typename T> T *take(size_t count) {
+        off = (off + 255) & ~(size_t)255;
+        T *p = reinterpret_cast<T *>(base + off);
+        off += count * sizeof(T);
+        return p;
+    }
+    static size_t need(std::initializer_list<size_t> bytes) {
+        size_t s = 0;
+        for (size_t b : bytes)
+            s += ((b + 255) & ~(size_t)255) + 256;
+        return s;
+    }
+};
+
+// Sorted unique u64 keys -> CSR in g.
+beep_status keys_to_graph(Ctx *ctx, Graph *g, uint64_t *keys, uint64_t *keys_tmp, int64_t nkeys, int64_t n) {
+    cudaStream_t s = ctx->stream;
+    // sort
+    int end_bit = 64;
+    size_t tb = 0;
+    BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys, keys_tmp, nkeys, 0, end_bit, s));
+    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(ctx->scratch.ptr, tb, keys, keys_tmp, nkeys, 0, end_bit, s));
+    // unique
+    BEEP_TRY(ctx->counter.reserve(64));
+    unsigned long long *d_num = ctx->counter.as<unsigned long long>();
+    tb = 0;
+    BEEP_CUDA_TRY(cub::DeviceSelect::Unique(nullptr, tb, keys_tmp, keys, d_num, nkeys, s));
+    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_CUDA_TRY(cub::DeviceSelect::Unique(ctx->scratch.ptr, tb, keys_tmp, keys, d_num, nkeys, s));
+    unsigned long long h_num = 0;
+    BEEP_CUDA_TRY(cudaMemcpyAsync(&h_num, d_num, sizeof(h_num), cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    int64_t m = (int64_t)h_num;
+    if (m > 0) {
+        uint64_t last = 0;
+        BEEP_CUDA_TRY(cudaMemcpyAsync(&last, keys + (m - 1), sizeof(last), cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+        if (last == ~0ull)
+            --m; // self-loop sentinel
+    }
+    if (m >= (int64_t)0xffffffffll)
+        return fail(BEEP_ERR_UNSUPPORTED, "graph has 2^32 or more directed edges");
+    g->n = n;
+    g->m = m;
+    BEEP_TRY(g->row_ptr.reserve((size_t)(n + 1) * 4));
+    BEEP_TRY(g->col.reserve((size_t)(m > 0 ? m : 1) * 4));
+    uint32_t *deg = g->row_ptr.as<uint32_t>();
+    BEEP_CUDA_TRY(cudaMemsetAsync(deg, 0, (size_t)(n + 1) * 4, s));
+    if (m > 0)
+        k_keys_to_coo<<<grid_for(m, 256, ctx->num_sms), 256, 0, s>>>(keys, m, g->col.as<uint32_t>(), deg);
+        ++ctx->launches;
+    BEEP_CUDA_TRY(cudaGetLastError());
+    tb = 0;
+    BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, deg, n + 1, s));
+    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ctx->scratch.ptr, tb, deg, deg, n + 1, s));
+    return BEEP_OK;
+}
+
+beep_status finish_graph(Ctx *ctx, Graph *g) {
+    cudaStream_t s = ctx->stream;
+    BEEP_TRY(ctx->counter.reserve(64));
+    unsigned long long *d = ctx->counter.as<unsigned long long>();
+    BEEP_CUDA_TRY(cudaMemsetAsync(d, 0, 16, s));
+    if (g->n > 0)
+        k_degree_stats<<<grid_for(g->n, 256, ctx->num_sms), 256, 0, s>>>(g->row_ptr.as<uint32_t>(), g->n, d,
+                                                                         reinterpret_cast<unsigned *>(d + 1));
+    BEEP_CUDA_TRY(cudaGetLastError());
+    unsigned long long h[2] = {0, 0};
+    BEEP_CUDA_TRY(cudaMemcpyAsync(h, d, 16, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    g->max_degree = (int64_t)(uint32_t)h[1];
+    // cutoff = ceil(mean + 6 sd) over all n vertices (include/utils.cuh:241-260)
+    if (g->n > 0) {
+        const double n = (double)g->n;
+        const double mean = (double)g->m / n;
+        double var = (double)h[0] / n - mean * mean;
+        if (var < 0)
+            var = 0;
+        g->cutoff = (uint32_t)std::ceil(mean + 6.0 * std::sqrt(var));
+    } else {
+        g->cutoff = 0;
+    }
+    g->views.clear();
+    return BEEP_OK;
+}
+
+} // namespace
+
+beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m, const uint32_t *d_rp,
+                                        const uint32_t *d_col) {
+    cudaStream_t s = ctx->stream;
+    if (n < 0 || m < 0 || n >= (int64_t)0xffffffffll || m >= (int64_t)0xffffffffll)
+        return fail(BEEP_ERR_INVALID_ARG, "graph size out of range");
+    // Fast path: rows already strictly increasing with no self loop.
+    BEEP_TRY(ctx->counter.reserve(64));
+    unsigned *d_bad = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 32);
+    BEEP_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 4, s));
+    if (n > 0)
+        k_check_csr<<<grid_for(n * 32, 256, ctx->num_sms), 256, 0, s>>>(d_rp, d_col, n, m, d_bad);
+        ++ctx->launches;
+    BEEP_CUDA_TRY(cudaGetLastError());
+    unsigned h_bad = 0;
+    uint32_t h_m_end = 0;
+    BEEP_CUDA_TRY(cudaMemcpyAsync(&h_bad, d_bad, 4, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaMemcpyAsync(&h_m_end, d_rp + n, 4, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    if ((int64_t)h_m_end != m)
+        return fail(BEEP_ERR_INVALID_ARG, "row_ptr[n] != m");
+    if (!h_bad) {
+        g->n = n;
+        g->m = m;
+        BEEP_TRY(g->row_ptr.reserve((size_t)(n + 1) * 4));
+        BEEP_TRY(g->col.reserve((size_t)(m > 0 ? m : 1) * 4));
+        if (g->row_ptr.ptr != (const void *)d_rp)
+            BEEP_CUDA_TRY(cudaMemcpyAsync(g->row_ptr.ptr, d_rp, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, s));
+        if (m > 0 && g->col.ptr != (const void *)d_col)
+            BEEP_CUDA_TRY(cudaMemcpyAsync(g->col.ptr, d_col, (size_t)m * 4, cudaMemcpyDeviceToDevice, s));
+        return finish_graph(ctx, g);
+    }
+    // Slow path: sort + unique packed (src, dst) keys. Out-of-range ids fail.
+    DevBuf keys, keys2;
+    BEEP_TRY(keys.reserve((size_t)(m > 0 ? m : 1) * 8));
+    BEEP_TRY(keys2.reserve((size_t)(m > 0 ? m : 1) * 8));
+    if (n > 0)
+        k_csr_keys<<<grid_for(n * 32, 256, ctx->num_sms), 256, 0, s>>>(d_rp, d_col, n, keys.as<uint64_t>());
+        ++ctx->launches;
+    BEEP_CUDA_TRY(cudaGetLastError());
+    BEEP_TRY(keys_to_graph(ctx, g, keys.as<uint64_t>(), keys2.as<uint64_t>(), m, n));
+    // validate ids
+    if (g->m > 0) {
+        uint32_t maxc = 0;
+        size_t tb = 0;
+        unsigned *d_max = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 40);
+        BEEP_CUDA_TRY(cub::DeviceReduce::Max(nullptr, tb, g->col.as<uint32_t>(), d_max, g->m, s));
+        BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+        BEEP_CUDA_TRY(cub::DeviceReduce::Max(ctx->scratch.ptr, tb, g->col.as<uint32_t>(), d_max, g->m, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(&maxc, d_max, 4, cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+        if ((int64_t)maxc >= n)
+            return fail(BEEP_ERR_INVALID_ARG, "column index >= n");
+    }
+    return finish_graph(ctx, g);
+}
+
+beep_status graph_build_from_device_edges(Ctx *ctx, Graph *g, int64_t ne, const uint32_t *d_src,
+                                          const uint32_t *d_dst) {
+    cudaStream_t s = ctx->stream;
+    if (ne < 0 || ne >= (int64_t)0xffffffffll)
+        return fail(BEEP_ERR_INVALID_ARG, "edge count out of range");
+    DevBuf keys, keys2;
+    BEEP_TRY(keys.reserve((size_t)(ne > 0 ? ne : 1) * 8));
+    BEEP_TRY(keys2.reserve((size_t)(ne > 0 ? ne : 1) * 8));
+    BEEP_TRY(ctx->counter.reserve(64));
+    unsigned *d_max = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 48);
+    BEEP_CUDA_TRY(cudaMemsetAsync(d_max, 0, 4, s));
+    if (ne > 0)
+        k_edge_keys<<<grid_for(ne, 256, ctx->num_sms), 256, 0, s>>>(d_src, d_dst, ne, keys.as<uint64_t>(), d_max);
+        ++ctx->launches;
+    BEEP_CUDA_TRY(cudaGetLastError());
+    unsigned h_max = 0;
+    BEEP_CUDA_TRY(cudaMemcpyAsync(&h_max, d_max, 4, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    int64_t n = ne > 0 ? (int64_t)h_max + 1 : 0;
+    BEEP_TRY(keys_to_graph(ctx, g, keys.as<uint64_t>(), keys2.as<uint64_t>(), ne, n));
+    return finish_graph(ctx, g);
+}
+
+namespace {
+
+beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *v) {
+    cudaStream_t s = ctx->stream;
+    const int64_t n = g->n, m = g->m;
+    v->min_qdeg = min_qdeg;
+    v->asc = asc;
+    const uint32_t *rp = g->row_ptr.as<uint32_t>();
+    const uint32_t *col = g->col.as<uint32_t>();
+    const int64_t nn = n > 0 ? n : 1;
+    size_t need = Carve::need({(size_t)nn * 4, (size_t)nn, (size_t)nn * 4, (size_t)nn * 8, (size_t)nn * 8,
+                               (size_t)nn * 4, (size_t)(m > 0 ? m : 1) * 4});
+    BEEP_TRY(ctx->scratch2.reserve(need));
+    Carve cv(ctx->scratch2.ptr);
+    uint32_t *deg = cv.take<uint32_t>(nn);
+    uint8_t *alive = cv.take<uint8_t>(nn);
+    uint32_t *rank = cv.take<uint32_t>(nn);
+    uint64_t *keys = cv.take<uint64_t>(nn);
+    uint64_t *keys2 = cv.take<uint64_t>(nn);
+    uint32_t *new_deg = cv.take<uint32_t>(nn);
+    uint32_t *col_tmp = cv.take<uint32_t>(m > 0 ? m : 1);
+    BEEP_TRY(ctx->counter.reserve(64));
+    unsigned long long *d_removed = ctx->counter.as<unsigned long long>();
+
+    const int gv = grid_for(n, 256, ctx->num_sms);
+    const int gw = grid_for(n * 32, 256, ctx->num_sms);
+    if (n > 0)
+        k_peel_init<<<gv, 256, 0, s>>>(rp, n, deg, alive);
+        ++ctx->launches;
+    BEEP_CUDA_TRY(cudaGetLastError());
+    // Iterated peel: loop while a round removes more than 5% of n
+    // (subgraph_matching.cuh:699-758).
+    int rounds = 0;
+    for (;;) {
+        unsigned long long removed = 0;
+        if (min_qdeg > 1 && n > 0) {
+            BEEP_CUDA_TRY(cudaMemsetAsync(d_removed, 0, 8, s));
+            k_peel_mark<<<gv, 256, 0, s>>>(deg, alive, n, (uint32_t)min_qdeg, d_removed);
+            ++ctx->launches;
+            BEEP_CUDA_TRY(cudaGetLastError());
+            BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, d_removed, 8, cudaMemcpyDeviceToHost, s));
+            BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+            removed = ctx->h_pinned[0];
+            if (removed > 0)
+                k_peel_degree<<<gw, 256, 0, s>>>(rp, col, alive, n, deg);
+                ++ctx->launches;
+            BEEP_CUDA_TRY(cudaGetLastError());
+        }
+        ++rounds;
+        if (!((double)removed > 0.05 * (double)n))
+            break;
+    }
+    v->peel_rounds = rounds;
+
+    // Relabel by priority.
+    const uint32_t maxdeg = (uint32_t)g->max_degree;
+    int hb = 1;
+    while (hb < 32 && ((uint64_t)1 << hb) <= (uint64_t)maxdeg)
+        ++hb;
+    unsigned long long *d_alive = d_removed + 1;
+    BEEP_CUDA_TRY(cudaMemsetAsync(d_alive, 0, 8, s));
+    if (n > 0)
+        k_prio_keys<<<gv, 256, 0, s>>>(deg, n, maxdeg, asc, keys, d_alive);
+        ++ctx->launches;
+    BEEP_CUDA_TRY(cudaGetLastError());
+    size_t tb = 0;
+    BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys, keys2, n, 0, 32 + hb, s));
+    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(ctx->scratch.ptr, tb, keys, keys2, n, 0, 32 + hb, s));
+    // number of vertices that kept an edge
+    BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, d_alive, 8, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    const int64_t na = (int64_t)ctx->h_pinned[0];
+    v->n = na;
+    BEEP_TRY(v->row_ptr.reserve((size_t)(na + 1) * 4));
+    BEEP_TRY(v->orig.reserve((size_t)(na > 0 ? na : 1) * 4));
+    BEEP_TRY(v->split.reserve((size_t)(na > 0 ? na : 1) * 4));
+    BEEP_CUDA_TRY(cudaMemsetAsync(rank, 0xff, (size_t)nn * 4, s));
+    BEEP_CUDA_TRY(cudaMemsetAsync(new_deg, 0, (size_t)nn * 4, s));
+    if (na > 0)
+        k_rank<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(keys2, na, v->orig.as<uint32_t>(), rank, deg,
+                                                               new_deg);
+    BEEP_CUDA_TRY(cudaGetLastError());
+    uint32_t *nrp = v->row_ptr.as<uint32_t>();
+    tb = 0;
+    BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, new_deg, nrp, na + 1, s));
+    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ctx->scratch.ptr, tb, new_deg, nrp, na + 1, s));
+    uint32_t h_m = 0;
+    BEEP_CUDA_TRY(cudaMemcpyAsync(&h_m, nrp + na, 4, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    v->m = h_m;
+    BEEP_TRY(v->col.reserve((size_t)(h_m > 0 ? h_m : 1) * 4));
+    if (na > 0)
+        k_fill_rows<<<grid_for(na * 32, 256, ctx->num_sms), 256, 0, s>>>(rp, col, v->orig.as<uint32_t>(), rank,
+                                                                           nrp, na, col_tmp);
+    BEEP_CUDA_TRY(cudaGetLastError());
+    if (h_m > 0) {
+        tb = 0;
+        BEEP_CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(nullptr, tb, col_tmp, v->col.as<uint32_t>(), (int64_t)h_m,
+                                                         na, nrp, nrp + 1, s));
+        BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+        BEEP_CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(ctx->scratch.ptr, tb, col_tmp, v->col.as<uint32_t>(),
+                                                         (int64_t)h_m, na, nrp, nrp + 1, s));
+    }
+    if (na > 0)
+        k_split<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(nrp, v->col.as<uint32_t>(), na,
+                                                                v->split.as<uint32_t>());
+    BEEP_CUDA_TRY(cudaGetLastError());
+    // max degree of the view
+    {
+        uint32_t *d_mx = reinterpret_cast<uint32_t *>(d_removed + 2);
+        BEEP_CUDA_TRY(cudaMemsetAsync(d_mx, 0, 4, s));
+        tb = 0;
+        BEEP_CUDA_TRY(cub::DeviceReduce::Max(nullptr, tb, new_deg, d_mx, na > 0 ? na : 1, s));
+        BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+        BEEP_CUDA_TRY(cub::DeviceReduce::Max(ctx->scratch.ptr, tb, new_deg, d_mx, na > 0 ? na : 1, s));
+        uint32_t mx = 0;
+        BEEP_CUDA_TRY(cudaMemcpyAsync(&mx, d_mx, 4, cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+        v->max_deg = (int32_t)mx;
+    }
+    return BEEP_OK;
+}
+
+} // namespace
+
+beep_status get_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, bool no_cache, View **out, bool *built,
+                     cudaEvent_t) {
+    auto key = std::make_pair((int)min_qdeg, (int)asc);
+    if (no_cache)
+        g->views.erase(key);
+    auto it = g->views.find(key);
+    if (it != g->views.end()) {
+        *out = it->second.get();
+        if (built)
+            *built = false;
+        return BEEP_OK;
+    }
+    auto v = std::make_unique<View>();
+    BEEP_TRY(build_view(ctx, g, min_qdeg, asc, v.get()));
+    *out = v.get();
+    g->views[key] = std::move(v);
+    if (built)
+        *built = true;
+    return BEEP_OK;
+}
+
+} // namespace beep

@@ -1,0 +1,180 @@
+// internal.h — shared host/device declarations of the B200 subgraph library.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/beep.h"
+
+namespace beep {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+void set_error(const std::string &msg);
+beep_status fail(beep_status s, const std::string &msg);
+
+#define BEEP_CUDA_TRY(expr)                                                                        \
+    do {                                                                                           \
+        cudaError_t e__ = (expr);                                                                  \
+        if (e__ != cudaSuccess) {                                                                  \
+            return ::beep::fail(e__ == cudaErrorMemoryAllocation ? BEEP_ERR_OUT_OF_MEMORY            \
+                                                                 : BEEP_ERR_CUDA,                  \
+                                std::string(#expr) + ": " + cudaGetErrorString(e__));              \
+        }                                                                                          \
+    } while (0)
+
+#define BEEP_TRY(expr)                                                                             \
+    do {                                                                                           \
+        beep_status s__ = (expr);                                                                  \
+        if (s__ != BEEP_OK)                                                                        \
+            return s__;                                                                            \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// compiled query plan
+// ---------------------------------------------------------------------------
+constexpr int kMaxQ = BEEP_MAX_QUERY;
+
+// The plan as the kernels consume it (passed by value as a kernel argument).
+struct DevPlan {
+    int32_t K;               // query vertices
+    int32_t dend;            // positions matched: K (sgm) or K - LUNMAT (sgc)
+    uint32_t back[kMaxQ];    // bit q (q >= 1): position q is a back edge of position p
+    uint32_t sym[kMaxQ];     // bit s (s >= 1): x_p > x_s is required
+    int32_t order[kMaxQ];    // query vertex at each position
+    int32_t pos1_after_root; // position 1 must follow the root in the priority order
+    int32_t restricted;      // every position follows the root: search only the out-list
+    int32_t asc;             // ascending (degree, id) priority order
+    int32_t pad;
+};
+
+struct QueryPlan {
+    beep_plan_info info;     // the reference-visible plan (per mode)
+    DevPlan dev;
+};
+
+// Compile the plan of a query CSR (qn vertices) for a mode.
+beep_status compile_plan(int32_t qn, const std::vector<int32_t> &qrow_ptr, const std::vector<int32_t> &qcol,
+                         beep_mode mode, QueryPlan *out);
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    // Grow-only: keeps the allocation when it is already large enough.
+    beep_status reserve(size_t b) {
+        if (b <= bytes && ptr)
+            return BEEP_OK;
+        release();
+        if (b == 0)
+            b = 16;
+        cudaError_t e = cudaMalloc(&ptr, b);
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            return fail(BEEP_ERR_OUT_OF_MEMORY, std::string("cudaMalloc ") + std::to_string(b) + " bytes: " +
+                                                    cudaGetErrorString(e));
+        }
+        bytes = b;
+        return BEEP_OK;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// A peeled, priority-relabelled copy of the graph for one (min_qdeg, order).
+// New ids follow the reference's priority order, so each sorted row is the
+// reference's oriented_colInd row (subgraph_matching.cuh:1282-1336).
+struct View {
+    int32_t min_qdeg = 0;
+    int32_t asc = 1;
+    int64_t n = 0;           // vertices with degree > 0 after peeling
+    int64_t m = 0;           // directed edges
+    int32_t max_deg = 0;
+    int32_t peel_rounds = 0;
+    DevBuf row_ptr;          // u32[n+1]
+    DevBuf col;              // u32[m], new ids, rows ascending
+    DevBuf orig;             // u32[n]: new id -> input id
+    DevBuf split;            // u32[n]: neighbours with a smaller new id
+};
+
+struct Graph {
+    int device = 0;
+    int64_t n = 0, m = 0;
+    int64_t max_degree = 0;
+    uint32_t cutoff = 0;
+    DevBuf row_ptr; // u32[n+1]
+    DevBuf col;     // u32[m]
+    std::map<std::pair<int, int>, std::unique_ptr<View>> views;
+};
+
+struct Query {
+    int32_t qn = 0;
+    std::vector<int32_t> row_ptr, col; // query CSR as CSRCOO::from_edgelist builds it
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    double wait_timeout_ms = 1000.0;
+    int num_sms = 148;
+    size_t smem_optin = 0;
+    DevBuf scratch;      // CUB temp storage and small per-call arrays
+    DevBuf scratch2;
+    DevBuf arena;        // neighbourhood bitmaps of large roots
+    DevBuf counter;      // u64 counters
+    unsigned long long *h_pinned = nullptr; // pinned host mirror of small results
+    uint64_t launches = 0; // kernels of this library launched on the context
+};
+
+// device entry points (device.cu)
+beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m, const uint32_t *d_row_ptr,
+                                        const uint32_t *d_col);
+beep_status graph_build_from_device_edges(Ctx *ctx, Graph *g, int64_t n_edges, const uint32_t *d_src,
+                                          const uint32_t *d_dst);
+beep_status get_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, bool no_cache, View **out,
+                     bool *built, cudaEvent_t ev_begin);
+
+struct EnumRequest {
+    uint64_t k = 0;
+    int32_t *d_out = nullptr;  // k*K ints on the device
+};
+
+beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t options, const EnumRequest *en,
+                      beep_stats *stats);
+
+// host helpers (io.cpp)
+beep_status read_bel(const char *path, std::vector<uint32_t> &src, std::vector<uint32_t> &dst);
+beep_status read_mtx(const char *path, std::vector<int32_t> &src, std::vector<int32_t> &dst);
+beep_status query_from_edges(const std::vector<int32_t> &src, const std::vector<int32_t> &dst, Query *q);
+
+} // namespace beep
+
+struct beep_ctx {
+    beep::Ctx impl;
+};
+struct beep_graph {
+    beep::Graph impl;
+    beep_ctx *ctx = nullptr;
+};
+struct beep_query {
+    beep::Query impl;
+};

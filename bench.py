@@ -1,0 +1,399 @@
+"""Benchmark: exact subgraph counting throughput (matches/s) on B200.
+
+Workload (default, "plain, mid"): R-MAT scale 20, edge factor 3,
+(a, b, c) = (0.57, 0.19, 0.19), seed 7 (loops and duplicates removed,
+int32 CSR with both directions); one step = device build of the graph from
+the resident CSR, then exact counts of the 4-clique and the diamond (sgm),
+each including its peel and priority relabelling.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value: total matches counted per second with the CSR resident in HBM (device
+time over K steps, CUDA events on the library's stream, L2 flushed between
+steps). e2e: the same through the public API from pinned host buffers,
+host->device copy of the CSR and the count read-back inside the timed region.
+Under torchrun each rank counts its own replica of the workload (no
+collective on the data path); times are max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "matches/sec on 1 B200 (exact counts), batched/served vs plain; p50/p99 latency"
+UNIT = "matches/s"
+
+WORKLOADS = {
+    "c2": {"desc": "plain-mid: R-MAT s20 ef3 seed 7; 4-clique + diamond (sgm)",
+           "graph": ("rmat", (20, 3, 0.57, 0.19, 0.19, 7)), "patterns": ["k4", "diamond"], "mode": "sgm"},
+    "c1": {"desc": "plain-small: ER G(4096, 0.004) seed 1; triangle (sgc)",
+           "graph": ("er", (4096, 0.004, 1)), "patterns": ["triangle"], "mode": "sgc"},
+}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def gen_graph(kind, args):
+    import beep_b200 as B
+
+    if kind == "rmat":
+        return B.gen_rmat(*args)
+    if kind == "er":
+        return B.gen_erdos_renyi(*args)
+    if kind == "cl":
+        return B.gen_chung_lu(*args)
+    raise ValueError(kind)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (OpenMP port of the reference algorithm) on the
+# host cores, on the same workload
+# ---------------------------------------------------------------------------
+def cpu_baseline(rp, col, wl, budget_s: float = 20.0) -> dict:
+    from beep_b200 import patterns as P
+    from oracle import pyoracle as O
+
+    threads = os.cpu_count() or 1
+    sgc = wl["mode"] == "sgc"
+    t0 = time.perf_counter()
+    total = 0
+    for name in wl["patterns"]:
+        total += O.count(rp, col, P.NAMED[name], sgc=sgc, threads=threads)["count"]
+    dt = time.perf_counter() - t0
+    runs = 1
+    # repeat the full workload while it stays inside the time budget
+    while dt / runs * (runs + 1) < budget_s and runs < 5:
+        for name in wl["patterns"]:
+            O.count(rp, col, P.NAMED[name], sgc=sgc, threads=threads)
+        runs += 1
+        dt = time.perf_counter() - t0
+    return {"value": total * runs / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"full workload ({' + '.join(wl['patterns'])}, all roots) x{runs}, {dt:.1f} s, "
+                      f"OpenMP oracle on {threads} host threads"}
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference_binary(binary, bel, mtx, mode, timeout):
+    r = subprocess.run([binary, "-g", bel, "-t", mtx, "-m", mode, "-d", "0"], capture_output=True, text=True,
+                       timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference exited {r.returncode}: {r.stderr[-400:]}")
+    out = r.stdout
+    import re
+
+    cnt = re.search(r"Counter = (\d+)", out)
+    prep = re.search(r"Preprocessing TIME: ([0-9.eE+-]+) ms", out)
+    fin = re.search(r"final count time ([0-9.eE+-]+) s", out)
+    xfer = re.search(r"Transfer Time: ([0-9.eE+-]+) s", out)
+    if not cnt or not fin:
+        raise RuntimeError("reference output lacks the Counter / final count time lines")
+    t = float(fin.group(1)) + (float(prep.group(1)) / 1e3 if prep else 0.0) + (float(xfer.group(1)) if xfer else 0.0)
+    return int(cnt.group(1)), t
+
+
+def reference_arm(args, wl):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    import beep_b200 as B
+    from beep_b200 import patterns as P
+
+    rp, col = gen_graph(*wl["graph"])
+    binary = os.path.join(ROOT, "oracle", "_ref", "beep_ref")
+    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "config": {"workload": wl["desc"], "l2": "n/a (separate processes)"}}
+    if os.path.exists(binary) and not args.reference_port:
+        with tempfile.TemporaryDirectory() as td:
+            bel = os.path.join(td, "g.bel")
+            B.write_bel(bel, rp, col)
+            mtxs = {}
+            for name in wl["patterns"]:
+                mtxs[name] = os.path.join(td, f"{name}.mtx")
+                B.write_mtx(mtxs[name], P.NAMED[name])
+            times, counts = [], None
+            try:
+                for _ in range(args.steps):
+                    tot_t, cs = 0.0, []
+                    for name in wl["patterns"]:
+                        c, t = run_reference_binary(binary, bel, mtxs[name], wl["mode"], args.reference_timeout)
+                        cs.append(c)
+                        tot_t += t
+                    counts = cs
+                    times.append(tot_t)
+                med = statistics.median(times)
+                value = sum(counts) / med
+                line.update({"value": value, "ms_per_step": med * 1e3, "counts": dict(zip(wl["patterns"], counts)),
+                             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 0, "kind": "reference",
+                                              "sample": "reference sgm/sgc binary (src/main.cu built for sm_100a) "
+                                                        "on the B200; time = its Transfer + Preprocessing + final "
+                                                        "count lines"},
+                             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                     "d2h_bytes_per_step": 0}})
+                print(json.dumps(line), flush=True)
+                return
+            except (RuntimeError, subprocess.TimeoutExpired) as e:
+                line["reference_binary_error"] = str(e)[:300]
+    # CPU port of the reference algorithm
+    cb = cpu_baseline(rp, col, wl, budget_s=30.0)
+    line.update({"value": cb["value"], "ms_per_step": None, "cpu_baseline": cb,
+                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-port", action="store_true", help="reference arm: use the CPU port")
+    ap.add_argument("--reference-timeout", type=float, default=300.0)
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        reference_arm(args, wl)
+        return
+
+    world, rank, local = dist_setup()
+    import numpy as np
+    import torch
+
+    import beep_b200 as B
+    from beep_b200 import patterns as P
+
+    torch.cuda.set_device(local)
+    rp, col = gen_graph(*wl["graph"])
+    n, m = len(rp) - 1, len(col)
+    mode = B.SGC if wl["mode"] == "sgc" else B.SGM
+    stream = torch.cuda.Stream()
+    ctx = B.Context(local, cuda_stream=stream.cuda_stream)
+    queries = [B.Query.from_edges(P.NAMED[p]) for p in wl["patterns"]]
+    d_rp = torch.from_numpy(rp).cuda()
+    d_col = torch.from_numpy(col).cuda()
+    h_rp = torch.from_numpy(rp).pin_memory()
+    h_col = torch.from_numpy(col).pin_memory()
+    h_rp_np, h_col_np = h_rp.numpy(), h_col.numpy()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    torch.cuda.synchronize()
+
+    def step(host: bool):
+        if host:
+            g = B.Graph.from_csr(ctx, h_rp_np, h_col_np)
+        else:
+            g = B.Graph.from_device_csr(ctx, n, m, d_rp.data_ptr(), d_col.data_ptr())
+        total = 0
+        sts = []
+        for q in queries:
+            c, st = B.count(g, q, mode, B.OPT_TIMING if not host else 0, ctx=ctx, stats=True)
+            total += c
+            sts.append(st)
+        g.close()
+        return total, sts
+
+    def timed(host: bool, steps: int):
+        for _ in range(args.warmup):
+            step(host)
+        torch.cuda.synchronize()
+        barrier(world)
+        launches0 = ctx.kernel_launches()
+        with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            stream.synchronize()
+            e0.record(stream)
+            total, allst = 0, []
+            for _ in range(steps):
+                flush.fill_(1)
+                t, sts = step(host)
+                total += t
+                allst.append(sts)
+            e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = e0.elapsed_time(e1)
+        return total, ms, allst, ctx.kernel_launches() - launches0
+
+    clk = ClockSampler(local)
+    clk.start()
+    total, ms, allst, launches = timed(False, args.steps)
+    clocks = clk.stop()
+    ms = max_over_ranks(ms, world)
+    ms_step = ms / args.steps
+    per_step = total // args.steps
+    value = world * per_step / (ms_step / 1e3)
+
+    e_total, e_ms, _, _ = timed(True, args.steps)
+    e_ms = max_over_ranks(e_ms, world)
+    e2e_value = world * (e_total // args.steps) / (e_ms / args.steps / 1e3)
+
+    # dominant kernel of the counting phase and its adjacency bytes
+    tiers = {"small": ("small_ms", "small_bytes", "small_launches"),
+             "medium": ("medium_ms", "medium_bytes", "medium_launches"),
+             "large_dfs": ("large_dfs_ms", "large_bytes", "large_dfs_launches"),
+             "large_rows": ("large_encode_ms", "large_bytes", "large_encode_launches")}
+    agg = {k: [0.0, 0, 0] for k in tiers}
+    prep_ms = count_ms = 0.0
+    for sts in allst:
+        for st in sts:
+            prep_ms += st["prep_ms"]
+            count_ms += st["count_ms"]
+            for k, (tk, bk, lk) in tiers.items():
+                agg[k][0] += st[tk]
+                agg[k][1] += st[bk] if k != "large_rows" else 0
+                agg[k][2] += st[lk]
+    dom = max(agg, key=lambda k: agg[k][0])
+    dom_ms, dom_bytes, dom_launches = agg[dom]
+    if dom == "large_rows":
+        dom_bytes = sum(st["large_bytes"] for sts in allst for st in sts)
+    peak, peak_kind = peaks()
+    achieved = (dom_bytes / max(dom_launches, 1)) / ((dom_ms / max(dom_launches, 1)) / 1e3) / 1e9 if dom_ms else 0.0
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": wl["desc"], "n": n, "m_directed": m, "patterns": wl["patterns"], "mode": wl["mode"],
+                   "matches_per_step": per_step, "l2": "flushed (256 MB write) before every step",
+                   "step": "device CSR build + per-pattern peel/relabel + count"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * (n + 1) + 4 * m),
+                "d2h_bytes_per_step": 8 * len(queries) + 16, "ms_per_step": e_ms / args.steps},
+        "gpu_launches": int(launches),
+        "phases_ms_per_step": {"prep": prep_ms / args.steps, "count": count_ms / args.steps,
+                               **{k: v[0] / args.steps for k, v in agg.items()}},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                     else "fallback 6650 GB/s",
+                     "bytes_per_launch": dom_bytes / max(dom_launches, 1),
+                     "ms_per_launch": dom_ms / max(dom_launches, 1)},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(rp, col, wl)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,211 @@
+/*
+ * beep.h — C ABI of the B200 subgraph counting / enumeration library.
+ *
+ * This is the drop-in boundary for BEEP's `-m sgm` / `-m sgc` path. The
+ * reference exposes that path as a C++ template class
+ *   graph::SG_Match<uint>(MAINTASK task, ProcessBy by, int dev, uint cutoff, int ndev)
+ *   void SG_Match::run(COOCSRGraph_d<uint>& data, COOCSRGraph<uint>& query)
+ * (subgraph_matching/subgraph_matching.cuh:113-231) behind the CLI in
+ * src/main.cu:27-344, which loads the data graph from .bel
+ * (include/FIleReader.cuh:51-95), the query from .mtx
+ * (include/FIleReader.cuh:130-212, 299-353) and prints
+ * "------------- Counter = N" (subgraph_matching.cuh:1277).
+ *
+ * Conventions of this ABI:
+ *   - every call returns a beep_status; nothing exits, traps or aborts;
+ *     beep_last_error() gives the message of the last failure on the thread;
+ *   - device objects live behind opaque handles freed by *_destroy;
+ *   - inputs are never mutated (the reference frees and replaces the caller's
+ *     device CSR during peeling, subgraph_matching.cuh:746-756);
+ *   - one beep_ctx per host thread; all work of a context is ordered on its
+ *     CUDA stream.
+ */
+#ifndef BEEP_H
+#define BEEP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BEEP_MAX_QUERY 10 /* subgraph_matching/include/host_utils.cuh:10 (DEPTH) */
+
+typedef enum beep_status {
+    BEEP_OK = 0,
+    BEEP_ERR_INVALID_ARG = 1,   /* null pointer, bad size */
+    BEEP_ERR_IO = 2,            /* file cannot be opened / read */
+    BEEP_ERR_PARSE = 3,         /* malformed .mtx / .bel */
+    BEEP_ERR_UNSUPPORTED = 4,   /* query outside the supported class (no central vertex, K>10, ...) */
+    BEEP_ERR_CUDA = 5,          /* CUDA runtime error (message has the CUDA error string) */
+    BEEP_ERR_OUT_OF_MEMORY = 6, /* device or host allocation failed / admission refused */
+    BEEP_ERR_TIMEOUT = 7,       /* a bounded device wait ran out */
+    BEEP_ERR_INTERNAL = 8
+} beep_status;
+
+/* MAINTASK values GRAPH_MATCH ("sgm") and GRAPH_COUNT ("sgc")
+ * (include/defs.cuh:78-95, include/Config.h:80-84). */
+typedef enum beep_mode {
+    BEEP_MODE_SGM = 0, /* count every match (embeddings / |Aut(Q)|) */
+    BEEP_MODE_SGC = 1  /* reference sgc: when the last query position is not adjacent to
+                          the one before it (LUNMAT = 1), the count stops one level early
+                          (subgraph_matching.cuh:612-631, device_utils.cuh:253,303) */
+} beep_mode;
+
+typedef struct beep_ctx beep_ctx;
+typedef struct beep_graph beep_graph;
+typedef struct beep_query beep_query;
+
+/* ---- errors ------------------------------------------------------------ */
+
+/* Copies the last error message of the calling thread into buf (NUL
+ * terminated, truncated to len). Returns the full message length.
+ * Replaces the reference's fprintf + exit(1) in CUDA_RUNTIME
+ * (include/utils.cuh:27-40). */
+size_t beep_last_error(char *buf, size_t len);
+const char *beep_status_string(beep_status s);
+
+/* ---- context ----------------------------------------------------------- */
+
+/* Binds device `device` and a stream (NULL: the context creates its own).
+ * Replaces SG_Match's `dev` argument and cudaSetDevice
+ * (subgraph_matching.cuh:113, :180). */
+beep_status beep_ctx_create(int device, void *cuda_stream, beep_ctx **out);
+beep_status beep_ctx_destroy(beep_ctx *ctx);
+/* Bound (milliseconds) on every device-side wait of the context's kernels;
+ * a wait that runs out ends its kernel with BEEP_ERR_TIMEOUT. */
+beep_status beep_ctx_set_wait_timeout(beep_ctx *ctx, double ms);
+/* Number of the library's own kernels launched on this context so far. */
+beep_status beep_ctx_kernel_launches(const beep_ctx *ctx, uint64_t *out);
+
+/* ---- data graph -------------------------------------------------------- */
+
+/* Load a .bel edge list: 24-byte records {u64 dst, u64 src, u64 weight}
+ * (include/FIleReader.cuh:51-95 read_bel; src/main.cu:72-130,283-300).
+ * Self loops are dropped; duplicate edges are removed on the device. */
+beep_status beep_graph_load_bel(beep_ctx *ctx, const char *path, beep_graph **out);
+
+/* Build from a host CSR (both edge directions). Rows need not be sorted and
+ * may hold duplicates or self loops: the device build sorts, dedups and drops
+ * them. Replaces CSRCOO::from_edgelist + GPUArray::switch_to_gpu
+ * (include/CSRCOO.cuh:37-80, src/main.cu:106-126, 283-300). */
+beep_status beep_graph_from_csr(beep_ctx *ctx, int64_t n, int64_t m, const int32_t *row_ptr,
+                                const int32_t *col_ind, beep_graph **out);
+/* Same, from device pointers (copied into the graph; the caller keeps them). */
+beep_status beep_graph_from_device_csr(beep_ctx *ctx, int64_t n, int64_t m, const int32_t *d_row_ptr,
+                                       const int32_t *d_col_ind, beep_graph **out);
+/* Build from a host edge list (src[i] -> dst[i]); self loops dropped,
+ * duplicates removed, n = max id + 1 (include/CSRCOO.cuh:37-80). */
+beep_status beep_graph_from_edges(beep_ctx *ctx, int64_t n_edges, const uint32_t *src, const uint32_t *dst,
+                                  beep_graph **out);
+
+typedef struct beep_graph_info {
+    int64_t n;           /* vertices */
+    int64_t m;           /* directed edges after dedup */
+    int64_t max_degree;
+    uint32_t cutoff;     /* ceil(mean + 6*sd) of the degree (include/utils.cuh:186-261, src/main.cu:132) */
+    int32_t reserved;
+} beep_graph_info;
+beep_status beep_graph_info_get(const beep_graph *g, beep_graph_info *out);
+/* Copy the deduped CSR back to the host (row_ptr[n+1], col_ind[m]). */
+beep_status beep_graph_csr(const beep_graph *g, int32_t *row_ptr, int32_t *col_ind);
+beep_status beep_graph_destroy(beep_graph *g);
+
+/* ---- query ------------------------------------------------------------- */
+
+/* Load a .mtx query: '%' lines (a '%%' banner may say "symmetric"), a
+ * "rows cols nnz" line, then 0-based "row col" lines
+ * (include/FIleReader.cuh:130-212, 299-353; src/main.cu:310-334). */
+beep_status beep_query_load_mtx(const char *path, beep_query **out);
+/* From a directed edge list as the .mtx lists it (both directions). */
+beep_status beep_query_from_edges(int32_t n_edges, const int32_t *src, const int32_t *dst, beep_query **out);
+beep_status beep_query_destroy(beep_query *q);
+
+/* The compiled query plan (SG_Match::preprocess_query, detect_symmetry,
+ * check_unmat, detect_reuse's first_sym_level: subgraph_matching.cuh:257-631). */
+typedef struct beep_plan_info {
+    int32_t K;
+    int32_t order[BEEP_MAX_QUERY];                      /* query vertex at each position */
+    int32_t qdeg[BEEP_MAX_QUERY];
+    int32_t qedge_ptr[BEEP_MAX_QUERY + 1];              /* back edges (QEDGE / QEDGE_PTR) */
+    int32_t qedge[BEEP_MAX_QUERY * (BEEP_MAX_QUERY - 1) / 2];
+    int32_t sym_ptr[BEEP_MAX_QUERY + 1];                /* symmetry reps (SYMNODE / SYMNODE_PTR) */
+    int32_t sym[BEEP_MAX_QUERY * (BEEP_MAX_QUERY - 1) / 2];
+    int32_t unmat;                                      /* LUNMAT for the requested mode */
+    int32_t first_sym_level;
+    int32_t min_qdeg, max_qdeg;
+    int32_t aut_order;                                  /* |Aut(Q)| */
+    int32_t restricted;    /* 1: every position is ordered after the root, so only the
+                              root's higher-priority neighbours are searched */
+} beep_plan_info;
+beep_status beep_query_plan(const beep_query *q, beep_mode mode, beep_plan_info *out);
+
+/* ---- counting / enumeration -------------------------------------------- */
+
+enum {
+    /* Skip roots with degree >= 100*cutoff as the reference does
+     * (subgraph_matching.cuh:1052, 1098). Off by default: those roots are counted. */
+    BEEP_OPT_REFERENCE_ROOT_CAP = 1u << 0,
+    /* Record per-phase device times with CUDA events (beep_stats). */
+    BEEP_OPT_TIMING = 1u << 1,
+    /* Drop the graph's cached peeled/ordered views before running. */
+    BEEP_OPT_NO_VIEW_CACHE = 1u << 2
+};
+
+typedef struct beep_stats {
+    uint64_t count;
+    int64_t roots;              /* roots searched */
+    int64_t roots_small;        /* roots by kernel tier */
+    int64_t roots_medium;
+    int64_t roots_large;
+    int32_t peel_rounds;
+    int32_t ascending;          /* priority order used */
+    uint32_t cutoff;
+    int32_t kernel_launches;    /* kernels this call launched */
+    double prep_ms;             /* device time: peel + ordering (BEEP_OPT_TIMING) */
+    double count_ms;            /* device time: counting kernels */
+    double small_ms, medium_ms, large_encode_ms, large_dfs_ms;
+    int32_t small_launches, medium_launches, large_encode_launches, large_dfs_launches;
+    uint64_t adjacency_bytes;   /* adjacency bytes the kernels must read (roofline numerator) */
+    uint64_t bitmap_bytes;      /* neighbourhood bitmap bytes of the large tier */
+    uint64_t small_bytes, medium_bytes, large_bytes; /* adjacency_bytes by tier (BEEP_OPT_TIMING) */
+} beep_stats;
+
+/* Count matches. Replaces SG_Match::run + count_subgraphs + final_counter
+ * (subgraph_matching.cuh:178-231, 1038-1279; host_utils.cuh:318-321).
+ * stats may be NULL. */
+beep_status beep_count(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_mode mode, uint64_t *out_count);
+beep_status beep_count_ex(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t options,
+                          beep_stats *stats);
+
+/* Enumerate up to k full matches (sgm semantics) as int32 tuples of data
+ * vertex ids in ORIGINAL query-vertex order: out_tuples[i*K + v] is the data
+ * vertex matched to query vertex v. *n_out = min(k, total); *total_count
+ * (may be NULL) = the exact number of matches. Which matches are returned
+ * when k < total is unspecified. The reference only counts (its last level
+ * is a popcount, device_utils.cuh:303-306); this extends the same DFS. */
+beep_status beep_enumerate(beep_ctx *ctx, beep_graph *g, const beep_query *q, uint64_t k, int32_t *out_tuples,
+                           uint64_t *n_out, uint64_t *total_count);
+
+/* ---- synthetic inputs and files ---------------------------------------- */
+
+/* Deterministic generators (splitmix64 streams keyed by seed and edge index).
+ * Each writes an undirected simple graph as a CSR with both directions, rows
+ * sorted. Two-phase: call with row_ptr/col_ind NULL to get n and m, then
+ * with buffers of n+1 and m entries. */
+beep_status beep_gen_erdos_renyi(int64_t n, double p, uint64_t seed, int64_t *n_out, int64_t *m_out,
+                                 int32_t *row_ptr, int32_t *col_ind);
+beep_status beep_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed,
+                          int64_t *n_out, int64_t *m_out, int32_t *row_ptr, int32_t *col_ind);
+beep_status beep_gen_chung_lu(int64_t n, double avg_degree, double exponent, uint64_t seed, int64_t *n_out,
+                              int64_t *m_out, int32_t *row_ptr, int32_t *col_ind);
+
+/* Write a CSR as .bel (src-sorted, both directions) — the byte format
+ * read_bel consumes (include/FIleReader.cuh:63-89). */
+beep_status beep_write_bel(const char *path, int64_t n, const int32_t *row_ptr, const int32_t *col_ind);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BEEP_H */

@@ -1,0 +1,124 @@
+"""Pins the CPU oracle (the checker) against closed forms, brute force and
+the committed golden counts. CPU only."""
+import itertools
+import math
+
+import numpy as np
+import pytest
+
+from beep_b200 import patterns as P
+from oracle import pyoracle as O
+
+
+def csr_from_pairs(n, pairs):
+    adj = [set() for _ in range(n)]
+    for a, b in pairs:
+        if a != b:
+            adj[a].add(b)
+            adj[b].add(a)
+    rp = [0]
+    col = []
+    for v in range(n):
+        col += sorted(adj[v])
+        rp.append(len(col))
+    return np.array(rp, np.int64), np.array(col, np.int32)
+
+
+CLOSED = {
+    "triangle": lambda n: math.comb(n, 3),
+    "k4": lambda n: math.comb(n, 4),
+    "k5": lambda n: math.comb(n, 5),
+    "diamond": lambda n: 6 * math.comb(n, 4),
+    "tailed_triangle": lambda n: 12 * math.comb(n, 4),
+    "w5": lambda n: 15 * math.comb(n, 5),
+    "claw": lambda n: 4 * math.comb(n, 4),
+}
+
+
+@pytest.mark.parametrize("n", [5, 8, 13, 30])
+def test_complete_graph_closed_forms(built, n):
+    rp, col = csr_from_pairs(n, itertools.combinations(range(n), 2))
+    for name, q in P.NAMED.items():
+        assert O.count(rp, col, q, apply_root_cap=False)["count"] == CLOSED[name](n), name
+
+
+def test_bipartite_and_empty_have_no_triangles(built):
+    rp, col = csr_from_pairs(20, [(a, b) for a in range(10) for b in range(10, 20)])
+    for name in ["triangle", "k4", "diamond", "k5", "w5", "tailed_triangle"]:
+        assert O.count(rp, col, P.NAMED[name], apply_root_cap=False)["count"] == 0
+    # claw counts: each vertex of degree 10 has C(10,3) claws
+    assert O.count(rp, col, P.CLAW, apply_root_cap=False)["count"] == 20 * math.comb(10, 3)
+    rp, col = csr_from_pairs(5, [])
+    assert O.count(rp, col, P.TRIANGLE)["count"] == 0
+
+
+def test_random_graphs_match_brute_force(built):
+    rng = np.random.default_rng(11)
+    pats = list(P.NAMED.values()) + P.central_patterns(4) + P.central_patterns(5)
+    for _ in range(12):
+        n = int(rng.integers(6, 13))
+        p = float(rng.uniform(0.3, 0.8))
+        pairs = [(a, b) for a, b in itertools.combinations(range(n), 2) if rng.random() < p]
+        rp, col = csr_from_pairs(n, pairs)
+        for q in pats:
+            assert O.count(rp, col, q, apply_root_cap=False)["count"] == O.brute_force(rp, col, q)
+
+
+def test_sgc_unmat_semantics(built):
+    """sgc stops one level early when the last position is not adjacent to
+    the one before it (subgraph_matching.cuh:612-631): for the diamond it
+    counts (root, later neighbour, common neighbour) triples = 3 x triangles."""
+    n = 9
+    rp, col = csr_from_pairs(n, itertools.combinations(range(n), 2))
+    tri = O.count(rp, col, P.TRIANGLE)["count"]
+    assert O.plan(P.DIAMOND, sgc=True)["unmat"] == 1
+    assert O.count(rp, col, P.DIAMOND, sgc=True)["count"] == 3 * tri
+    # patterns whose last two positions are adjacent are unaffected
+    for name in ["triangle", "k4", "k5", "w5"]:
+        assert O.plan(P.NAMED[name], sgc=True)["unmat"] == 0
+        assert (O.count(rp, col, P.NAMED[name], sgc=True)["count"]
+                == O.count(rp, col, P.NAMED[name])["count"])
+
+
+def test_readme_triangle_plan(built):
+    """The README triangle (README.md:55-64): order 0,1,2, back edges
+    {},{0},{0,1}, symmetry chain 1>0, 2>0, 2>1, ascending order."""
+    p = O.plan(P.TRIANGLE)
+    assert p["order"] == [0, 1, 2]
+    assert p["qedge_ptr"] == [0, 0, 1, 3] and p["qedge"] == [0, 0, 1]
+    assert p["sym_ptr"] == [0, 0, 1, 3] and p["sym"] == [0, 0, 1]
+    assert p["first_sym_level"] == 2 and p["aut_order"] == 6
+
+
+def test_golden_small_fixtures(built, golden):
+    import beep_b200 as B
+
+    gens = {"er": B.gen_erdos_renyi, "cl": B.gen_chung_lu, "rmat": B.gen_rmat}
+    for gname, rec in golden["small"].items():
+        rp, col = gens[rec["kind"]](*rec["args"])
+        assert len(rp) - 1 == rec["n"] and len(col) == rec["m"]
+        for pname, c in rec["counts"].items():
+            q = [tuple(e) for e in golden["patterns"][pname]]
+            assert O.count(rp, col, q, apply_root_cap=False)["count"] == c["sgm"], (gname, pname)
+            assert O.count(rp, col, q, sgc=True, apply_root_cap=False)["count"] == c["sgc"], (gname, pname)
+
+
+def test_golden_c1(built, golden):
+    import beep_b200 as B
+
+    rec = golden["large"]["c1_er_4096_p004_s1"]
+    rp, col = B.gen_erdos_renyi(*rec["args"])
+    r = O.count(rp, col, P.TRIANGLE, sgc=True)
+    assert r["count"] == rec["counts"]["triangle"]["sgc"]
+    assert r["cutoff"] == rec["cutoff"]
+
+
+def test_peel_matches_definition(built):
+    """Iterated peel: rounds continue while more than 5% of n is removed."""
+    # a path 0-1-2-...-9 plus a triangle 10-11-12: min_qdeg 2 removes the path
+    # ends one layer per round
+    pairs = [(i, i + 1) for i in range(9)] + [(10, 11), (11, 12), (10, 12)]
+    rp, col = csr_from_pairs(13, pairs)
+    deg, alive, rounds = O.peel(rp, col, 2)
+    assert rounds >= 2
+    assert list(deg[10:13]) == [2, 2, 2]
