@@ -34,6 +34,7 @@ SGM, SGC = 0, 1
 OPT_REFERENCE_ROOT_CAP = 1 << 0
 OPT_TIMING = 1 << 1
 OPT_NO_VIEW_CACHE = 1 << 2
+OPT_ALG_BYTES = 1 << 3
 
 
 class BeepError(RuntimeError):

@@ -113,9 +113,8 @@ beep_status beep_ctx_create(int device, void *stream, beep_ctx **out) {
     return BEEP_OK;
 }
 
-beep_status beep_ctx_destroy(beep_ctx *ctx) {
-    if (!ctx)
-        return BEEP_OK;
+namespace {
+void ctx_free(beep_ctx *ctx) {
     cudaSetDevice(ctx->impl.device);
     cudaStreamSynchronize(ctx->impl.stream);
     ctx->impl.scratch.release();
@@ -127,6 +126,30 @@ beep_status beep_ctx_destroy(beep_ctx *ctx) {
     if (ctx->impl.own_stream)
         cudaStreamDestroy(ctx->impl.stream);
     delete ctx;
+}
+void ctx_release(beep_ctx *ctx) {
+    if (ctx && ctx->refs.fetch_sub(1) == 1)
+        ctx_free(ctx);
+}
+beep_graph *new_graph(beep_ctx *ctx) {
+    auto *g = new beep_graph;
+    g->ctx = ctx;
+    g->impl.device = ctx->impl.device;
+    ctx->refs.fetch_add(1);
+    return g;
+}
+void graph_free(beep_graph *g) {
+    beep_ctx *ctx = g->ctx;
+    cudaSetDevice(g->impl.device);
+    if (ctx)
+        cudaStreamSynchronize(ctx->impl.stream);
+    delete g;
+    ctx_release(ctx);
+}
+} // namespace
+
+beep_status beep_ctx_destroy(beep_ctx *ctx) {
+    ctx_release(ctx);
     return BEEP_OK;
 }
 
@@ -150,14 +173,12 @@ beep_status beep_graph_from_device_csr(beep_ctx *ctx, int64_t n, int64_t m, cons
         return fail(BEEP_ERR_INVALID_ARG, "beep_graph_from_device_csr: bad arguments");
     *out = nullptr;
     BEEP_TRY(bind(ctx));
-    auto *g = new beep_graph;
-    g->ctx = ctx;
-    g->impl.device = ctx->impl.device;
+    beep_graph *g = new_graph(ctx);
     beep_status s = graph_build_from_device_csr(&ctx->impl, &g->impl, n, m,
                                                 reinterpret_cast<const uint32_t *>(d_row_ptr),
                                                 reinterpret_cast<const uint32_t *>(d_col_ind));
     if (s != BEEP_OK) {
-        delete g;
+        graph_free(g);
         return s;
     }
     *out = g;
@@ -172,9 +193,7 @@ beep_status beep_graph_from_csr(beep_ctx *ctx, int64_t n, int64_t m, const int32
     if (row_ptr[0] != 0 || row_ptr[n] != m)
         return fail(BEEP_ERR_INVALID_ARG, "row_ptr must start at 0 and end at m");
     BEEP_TRY(bind(ctx));
-    auto *g = new beep_graph;
-    g->ctx = ctx;
-    g->impl.device = ctx->impl.device;
+    beep_graph *g = new_graph(ctx);
     // Upload straight into the graph's buffers; the build keeps them when the
     // rows are already sorted and simple.
     beep_status s = upload(&ctx->impl, g->impl.row_ptr, reinterpret_cast<const uint32_t *>(row_ptr), (size_t)n + 1);
@@ -184,7 +203,7 @@ beep_status beep_graph_from_csr(beep_ctx *ctx, int64_t n, int64_t m, const int32
         s = graph_build_from_device_csr(&ctx->impl, &g->impl, n, m, g->impl.row_ptr.as<uint32_t>(),
                                         g->impl.col.as<uint32_t>());
     if (s != BEEP_OK) {
-        delete g;
+        graph_free(g);
         return s;
     }
     *out = g;
@@ -200,13 +219,11 @@ beep_status beep_graph_from_edges(beep_ctx *ctx, int64_t n_edges, const uint32_t
     DevBuf ds, dd;
     BEEP_TRY(upload(&ctx->impl, ds, src, (size_t)n_edges));
     BEEP_TRY(upload(&ctx->impl, dd, dst, (size_t)n_edges));
-    auto *g = new beep_graph;
-    g->ctx = ctx;
-    g->impl.device = ctx->impl.device;
+    beep_graph *g = new_graph(ctx);
     beep_status s = graph_build_from_device_edges(&ctx->impl, &g->impl, n_edges, ds.as<uint32_t>(), dd.as<uint32_t>());
     cudaStreamSynchronize(ctx->impl.stream);
     if (s != BEEP_OK) {
-        delete g;
+        graph_free(g);
         return s;
     }
     *out = g;
@@ -245,13 +262,8 @@ beep_status beep_graph_csr(const beep_graph *g, int32_t *row_ptr, int32_t *col_i
 }
 
 beep_status beep_graph_destroy(beep_graph *g) {
-    if (!g)
-        return BEEP_OK;
-    if (g->ctx) {
-        cudaSetDevice(g->impl.device);
-        cudaStreamSynchronize(g->ctx->impl.stream);
-    }
-    delete g;
+    if (g)
+        graph_free(g);
     return BEEP_OK;
 }
 

@@ -931,7 +931,7 @@ beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t option
         st.kernel_launches += 1;
     }
     tm.stop(tcount, &st.count_ms);
-    if (tm.on) {
+    if (options & BEEP_OPT_ALG_BYTES) {
         k_alg_bytes<<<gv, 256, 0, s>>>(vd, pl, tier, n, d_cnt + 2);
         BEEP_CUDA_TRY(cudaGetLastError());
         st.kernel_launches += 1;

@@ -29,7 +29,7 @@ __global__ void k_check_csr(const uint32_t *__restrict__ rp, const uint32_t *__r
         const uint32_t b = rp[v], e = rp[v + 1];
         if (e < b || e > m) {
             if (lane == 0)
-                atomicOr(bad, 1u);
+                atomicOr(bad, 2u); // row pointers unusable
             continue;
         }
         for (uint32_t i = b + lane; i < e; i += 32) {
@@ -349,6 +349,8 @@ beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     if ((int64_t)h_m_end != m)
         return fail(BEEP_ERR_INVALID_ARG, "row_ptr[n] != m");
+    if (h_bad & 2u)
+        return fail(BEEP_ERR_INVALID_ARG, "row_ptr is not non-decreasing within [0, m]");
     if (!h_bad) {
         g->n = n;
         g->m = m;

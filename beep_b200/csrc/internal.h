@@ -1,6 +1,7 @@
 // internal.h — shared host/device declarations of the B200 subgraph library.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -168,8 +169,10 @@ beep_status query_from_edges(const std::vector<int32_t> &src, const std::vector<
 
 } // namespace beep
 
+// A context lives until its handle and every graph built on it are destroyed.
 struct beep_ctx {
     beep::Ctx impl;
+    std::atomic<int> refs{1};
 };
 struct beep_graph {
     beep::Graph impl;

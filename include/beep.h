@@ -150,7 +150,9 @@ enum {
     /* Record per-phase device times with CUDA events (beep_stats). */
     BEEP_OPT_TIMING = 1u << 1,
     /* Drop the graph's cached peeled/ordered views before running. */
-    BEEP_OPT_NO_VIEW_CACHE = 1u << 2
+    BEEP_OPT_NO_VIEW_CACHE = 1u << 2,
+    /* Compute the adjacency bytes of the searched roots (an extra pass). */
+    BEEP_OPT_ALG_BYTES = 1u << 3
 };
 
 typedef struct beep_stats {
@@ -167,9 +169,9 @@ typedef struct beep_stats {
     double count_ms;            /* device time: counting kernels */
     double small_ms, medium_ms, large_encode_ms, large_dfs_ms;
     int32_t small_launches, medium_launches, large_encode_launches, large_dfs_launches;
-    uint64_t adjacency_bytes;   /* adjacency bytes the kernels must read (roofline numerator) */
+    uint64_t adjacency_bytes;   /* adjacency bytes the kernels must read (BEEP_OPT_ALG_BYTES) */
     uint64_t bitmap_bytes;      /* neighbourhood bitmap bytes of the large tier */
-    uint64_t small_bytes, medium_bytes, large_bytes; /* adjacency_bytes by tier (BEEP_OPT_TIMING) */
+    uint64_t small_bytes, medium_bytes, large_bytes; /* adjacency_bytes by tier (BEEP_OPT_ALG_BYTES) */
 } beep_stats;
 
 /* Count matches. Replaces SG_Match::run + count_subgraphs + final_counter
