@@ -40,6 +40,7 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kSmallMaxD = 64;
+constexpr int kMediumAMaxD = 256;
 constexpr int kMediumMaxD = 1024;
 
 struct ViewDev {
@@ -263,6 +264,101 @@ __device__ __forceinline__ void make_ec(EnumCtx &ec, const EnumDev &en, const De
 }
 
 // ---------------------------------------------------------------------------
+// Row building, flattened over the elements to search so that every thread of
+// the group stays busy whatever the row lengths:
+//   1. per row i: the part of A[i]'s higher-priority list that lies inside
+//      [min, max] of the A entries it can meet (two binary searches);
+//   2. exclusive prefix of those lengths;
+//   3. each thread takes list elements t = tid, tid + nthr, ...: finds its row
+//      by binary search on the prefix, loads the element (consecutive t read
+//      consecutive addresses) and binary-searches it in A, setting both bits
+//      of every edge found.
+// Used by a warp (small tier), a block (medium tier) or a block on a chunk of
+// rows (large tier).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t upper_bound_g(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi,
+                                                  uint32_t key) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] <= key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Exclusive prefix of buf[0, R) in place, total in buf[R]; one warp.
+__device__ __forceinline__ void warp_excl_scan(uint32_t *buf, uint32_t R, int lane) {
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < R; base += 32) {
+        const uint32_t idx = base + lane;
+        const uint32_t x = idx < R ? buf[idx] : 0u;
+        uint32_t inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, inc, o);
+            if (lane >= o)
+                inc += y;
+        }
+        if (idx < R)
+            buf[idx] = carry + inc - x;
+        carry += __shfl_sync(kFull, inc, 31);
+    }
+    if (lane == 0)
+        buf[R] = carry;
+}
+
+template <bool BLOCK> __device__ __forceinline__ void group_sync() {
+    if constexpr (BLOCK)
+        __syncthreads();
+    else
+        __syncwarp();
+}
+
+template <bool BLOCK, typename SetFn>
+__device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const uint32_t *A, uint32_t D,
+                                                uint32_t i0, uint32_t i1, uint32_t *s_hb, uint32_t *s_pre,
+                                                uint32_t tid, uint32_t nthr, SetFn set) {
+    const uint32_t R = i1 - i0;
+    for (uint32_t r = tid; r < R; r += nthr) {
+        const uint32_t i = i0 + r;
+        uint32_t hb, he, xb, xe, c = 0;
+        hd_range(v, asc, A[i], i, D, hb, he, xb, xe);
+        if (xb < xe && hb < he) {
+            const uint32_t lo = lower_bound_g(v.col, hb, he, A[xb]);
+            const uint32_t hi = upper_bound_g(v.col, lo, he, A[xe - 1]);
+            hb = lo;
+            c = hi - lo;
+        }
+        s_hb[r] = hb;
+        s_pre[r] = c;
+    }
+    group_sync<BLOCK>();
+    if (tid < 32)
+        warp_excl_scan(s_pre, R, (int)tid);
+    group_sync<BLOCK>();
+    const uint32_t T = s_pre[R];
+    for (uint32_t t = tid; t < T; t += nthr) {
+        // row r: last with s_pre[r] <= t
+        uint32_t lo = 0, hi = R;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_pre[mid] <= t)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const uint32_t i = i0 + lo;
+        const uint32_t w = v.col[s_hb[lo] + (t - s_pre[lo])];
+        const uint32_t xb = asc ? i + 1 : 0, xe = asc ? D : i;
+        const int k = find_idx(A, xb, xe, w);
+        if (k >= 0)
+            set(i, (uint32_t)k);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // small tier: warp per root
 // ---------------------------------------------------------------------------
 constexpr int kSmallWarps = 8;
@@ -273,6 +369,8 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(ViewDev v, DevPlan p
                                                            EnumDev en) {
     __shared__ uint64_t s_rows[kSmallWarps][kSmallMaxD];
     __shared__ uint32_t s_A[kSmallWarps][kSmallMaxD];
+    __shared__ uint32_t s_hb[kSmallWarps][kSmallMaxD];
+    __shared__ uint32_t s_pre[kSmallWarps][kSmallMaxD + 1];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const Lp lp = load_lp(pl);
     uint64_t *rows = s_rows[wib];
@@ -290,25 +388,11 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(ViewDev v, DevPlan p
             rows[i] = 0;
         }
         __syncwarp();
-        // rows: lane i searches the higher-priority list of A[i] against A
-        for (uint32_t i = lane; i < D; i += 32) {
-            uint32_t hb, he, xb, xe;
-            hd_range(v, pl.asc, A[i], i, D, hb, he, xb, xe);
-            if (xb >= xe || hb >= he)
-                continue;
-            const uint32_t amin = A[xb], amax = A[xe - 1];
-            hb = lower_bound_g(v.col, hb, he, amin);
-            for (uint32_t e = hb; e < he; ++e) {
-                const uint32_t w = v.col[e];
-                if (w > amax)
-                    break;
-                const int k = find_idx(A, xb, xe, w);
-                if (k >= 0) {
-                    atomicOr((unsigned long long *)&rows[i], 1ull << k);
-                    atomicOr((unsigned long long *)&rows[k], 1ull << i);
-                }
-            }
-        }
+        build_rows_flat<false>(v, pl.asc, A, D, 0, D, s_hb[wib], s_pre[wib], (uint32_t)lane, 32u,
+                               [&](uint32_t i, uint32_t k) {
+                                   atomicOr((unsigned long long *)&rows[i], 1ull << k);
+                                   atomicOr((unsigned long long *)&rows[k], 1ull << i);
+                               });
         __syncwarp();
         const uint64_t all = (D >= 64) ? ~0ull : ((1ull << D) - 1ull);
         if constexpr (ENUM) {
@@ -328,51 +412,21 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(ViewDev v, DevPlan p
 }
 
 // ---------------------------------------------------------------------------
-// row building shared by the medium and large tiers: one warp per row i;
-// lanes stride the higher-priority list of A[i] (coalesced) and search A.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void build_row_warp(const ViewDev &v, int asc, const uint32_t *A, uint32_t D, uint32_t i,
-                                               uint32_t *rows, uint32_t W, int lane) {
-    uint32_t hb, he, xb, xe;
-    hd_range(v, asc, A[i], i, D, hb, he, xb, xe);
-    if (xb >= xe || hb >= he)
-        return;
-    const uint32_t amin = A[xb], amax = A[xe - 1];
-    // skip the part of the list below A[xb] (one search per row)
-    if (lane == 0)
-        hb = lower_bound_g(v.col, hb, he, amin);
-    hb = __shfl_sync(kFull, hb, 0);
-    for (uint32_t base = hb; base < he; base += 32) {
-        const uint32_t e = base + lane;
-        uint32_t w = 0xffffffffu;
-        if (e < he)
-            w = v.col[e];
-        if (w <= amax) {
-            const int k = find_idx(A, xb, xe, w);
-            if (k >= 0) {
-                atomicOr(&rows[(size_t)i * W + ((uint32_t)k >> 5)], 1u << (k & 31));
-                atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
-            }
-        }
-        // the list is sorted: once every lane is past amax, stop
-        if (__all_sync(kFull, w > amax))
-            break;
-    }
-}
-
-// ---------------------------------------------------------------------------
 // medium tier: block per root, bitmap in shared memory
 // ---------------------------------------------------------------------------
 template <int DEND, bool ENUM>
-__global__ void __launch_bounds__(512) k_medium(ViewDev v, DevPlan pl, const uint32_t *__restrict__ roots,
+__global__ void __launch_bounds__(1024) k_medium(ViewDev v, DevPlan pl, const uint32_t *__restrict__ roots,
                                                 uint32_t nroots, int rev, unsigned *cursor,
                                                 unsigned long long *counter, EnumDev en, uint32_t maxD) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t s_ri, s_j;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
     const Lp lp = load_lp(pl);
+    const uint32_t pad = (maxD + 4) & ~3u;
     uint32_t *A = sm;
-    uint32_t *rows = sm + ((maxD + 3) & ~3u);
+    uint32_t *s_hb = sm + pad;
+    uint32_t *s_pre = sm + 2 * pad;
+    uint32_t *rows = sm + 3 * pad;
     EnumCtx ec;
     if constexpr (ENUM)
         make_ec(ec, en, pl, v);
@@ -395,8 +449,11 @@ __global__ void __launch_bounds__(512) k_medium(ViewDev v, DevPlan pl, const uin
         if (threadIdx.x == 0)
             s_j = j0;
         __syncthreads();
-        for (uint32_t i = wib; i < D; i += nw)
-            build_row_warp(v, pl.asc, A, D, i, rows, W, lane);
+        build_rows_flat<true>(v, pl.asc, A, D, 0, D, s_hb, s_pre, threadIdx.x, blockDim.x,
+                              [&](uint32_t i, uint32_t k) {
+                                  atomicOr(&rows[(size_t)i * W + (k >> 5)], 1u << (k & 31));
+                                  atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
+                              });
         __syncthreads();
         if constexpr (ENUM) {
             ec.A = A;
@@ -451,7 +508,7 @@ __global__ void __launch_bounds__(512) k_large_rows(ViewDev v, DevPlan pl, Batch
                                                     unsigned *cursor) {
     extern __shared__ __align__(16) uint32_t sA[];
     __shared__ uint32_t s_c;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ uint32_t s_hb[kRowsPerChunk], s_pre[kRowsPerChunk + 1];
     const uint32_t total = bt.cstart[bt.nb];
     for (;;) {
         if (threadIdx.x == 0)
@@ -475,8 +532,11 @@ __global__ void __launch_bounds__(512) k_large_rows(ViewDev v, DevPlan pl, Batch
             __syncthreads();
             A = sA;
         }
-        for (uint32_t i = i0 + wib; i < i1; i += nw)
-            build_row_warp(v, pl.asc, A, D, i, rows, W, lane);
+        build_rows_flat<true>(v, pl.asc, A, D, i0, i1, s_hb, s_pre, threadIdx.x, blockDim.x,
+                              [&](uint32_t i, uint32_t k) {
+                                  atomicOr(&rows[(size_t)i * W + (k >> 5)], 1u << (k & 31));
+                                  atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
+                              });
         __syncthreads();
     }
 }
@@ -519,11 +579,11 @@ __global__ void __launch_bounds__(256) k_large_dfs(ViewDev v, DevPlan pl, Batch 
 // ---------------------------------------------------------------------------
 // root classification
 // ---------------------------------------------------------------------------
-// tier: 0 none, 1 small, 2 medium, 3 large. Also accumulates the adjacency
+// tier: 0 none, 1 small, 2 medium (D <= 256), 3 medium (D <= 1024), 4 large. Also accumulates the adjacency
 // bytes the kernels must read for the roofline.
 __global__ void k_classify(ViewDev v, DevPlan pl, int64_t n, uint32_t min_deg, uint32_t cap_deg, uint8_t *tier,
                            uint32_t *dom, unsigned *tier_max) {
-    uint32_t mx[3] = {0, 0, 0};
+    uint32_t mx[4] = {0, 0, 0, 0};
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t deg = v.rp[r + 1] - v.rp[r];
         uint32_t beg, D, j0;
@@ -533,14 +593,14 @@ __global__ void k_classify(ViewDev v, DevPlan pl, int64_t n, uint32_t min_deg, u
         // enough domain vertices for the other dend-1 positions and at least
         // one level-1 vertex.
         if (deg >= min_deg && deg < cap_deg && D + 1 >= (uint32_t)pl.dend && j0 < D)
-            t = D <= kSmallMaxD ? 1 : (D <= kMediumMaxD ? 2 : 3);
+            t = D <= kSmallMaxD ? 1 : (D <= kMediumAMaxD ? 2 : (D <= kMediumMaxD ? 3 : 4));
         tier[r] = t;
         dom[r] = D;
         if (t)
             mx[t - 1] = max(mx[t - 1], D);
     }
 #pragma unroll
-    for (int t = 0; t < 3; ++t) {
+    for (int t = 0; t < 4; ++t) {
         const uint32_t m = __reduce_max_sync(kFull, mx[t]);
         if ((threadIdx.x & 31) == 0 && m)
             atomicMax(&tier_max[t], m);
@@ -578,7 +638,7 @@ __global__ void k_alg_bytes(ViewDev v, DevPlan pl, const uint8_t *__restrict__ t
             hd_range(v, pl.asc, v.col[beg + i], i, D, hb, he, xb, xe);
             a += 12ull + 4ull * (he - hb);
         }
-        acc[t - 1] += a;
+        acc[t == 1 ? 0 : (t == 4 ? 2 : 1)] += a;
     }
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
@@ -773,16 +833,16 @@ beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t option
     const int64_t n = v->n;
 
     // classify roots into tiers
-    size_t need = (size_t)n * 1 + 256 + (size_t)n * 4 * 6 + 4096;
+    size_t need = (size_t)n * 1 + 256 + (size_t)n * 4 * 8 + 4096;
     BEEP_TRY(ctx->scratch2.reserve(need));
     char *base = ctx->scratch2.as<char>();
     uint8_t *tier = reinterpret_cast<uint8_t *>(base);
     uint32_t *dom = reinterpret_cast<uint32_t *>(base + (((size_t)n + 255) & ~(size_t)255));
-    uint32_t *lists[3];
-    for (int t = 0; t < 3; ++t)
+    uint32_t *lists[4]; // small, medium (<= 256), medium (<= 1024), large
+    for (int t = 0; t < 4; ++t)
         lists[t] = dom + (size_t)n * (t + 1);
-    uint32_t *d_nsel = dom + (size_t)n * 4;       // [0..2] counts, [4..6] max domain per tier
-    uint32_t *d_gD = dom + (size_t)n * 4 + 64;     // large-tier gather
+    uint32_t *d_nsel = dom + (size_t)n * 5;       // [0..3] counts, [4..7] max domain per tier
+    uint32_t *d_gD = dom + (size_t)n * 5 + 64;     // large-tier gather
     uint32_t *d_gj = d_gD + (size_t)n;
     BEEP_CUDA_TRY(cudaMemsetAsync(d_nsel, 0, 64, s));
     uint64_t cap_deg = 0xffffffffull;
@@ -795,7 +855,7 @@ beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t option
     BEEP_CUDA_TRY(cudaGetLastError());
     st.kernel_launches += 1;
     uint32_t nsel[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int t = 0; t < 3; ++t) {
+    for (int t = 0; t < 4; ++t) {
         size_t tb = 0;
         cub::CountingInputIterator<uint32_t> it(0);
         TierSel sel{tier, (uint8_t)(t + 1)};
@@ -805,32 +865,32 @@ beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t option
         st.kernel_launches += 1;
     }
     BEEP_CUDA_TRY(cudaMemcpyAsync(nsel, d_nsel, sizeof(nsel), cudaMemcpyDeviceToHost, s));
-    const uint32_t max_medium = nsel[5];
+    const uint32_t max_medA = nsel[5], max_medB = nsel[6];
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     st.roots_small = nsel[0];
-    st.roots_medium = nsel[1];
-    st.roots_large = nsel[2];
-    st.roots = (int64_t)nsel[0] + nsel[1] + nsel[2];
+    st.roots_medium = (int64_t)nsel[1] + nsel[2];
+    st.roots_large = nsel[3];
+    st.roots = (int64_t)nsel[0] + nsel[1] + nsel[2] + nsel[3];
     // heaviest roots first: in ascending order they have the largest ids
     const int rev = pl.asc ? 1 : 0;
     BEEP_CUDA_TRY(cudaMemsetAsync(d_cursor, 0, 16, s));
 
     // large tier: batches of roots whose bitmaps fit the arena
-    if (nsel[2] > 0) {
-        std::vector<uint32_t> lr(nsel[2]), lD(nsel[2]), lj(nsel[2]);
-        k_gather_dom<<<std::max(1u, std::min(nsel[2] / 256 + 1, 1024u)), 256, 0, s>>>(vd, pl, lists[2], nsel[2], d_gD,
+    if (nsel[3] > 0) {
+        std::vector<uint32_t> lr(nsel[3]), lD(nsel[3]), lj(nsel[3]);
+        k_gather_dom<<<std::max(1u, std::min(nsel[3] / 256 + 1, 1024u)), 256, 0, s>>>(vd, pl, lists[3], nsel[3], d_gD,
                                                                                       d_gj);
         BEEP_CUDA_TRY(cudaGetLastError());
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lr.data(), lists[2], 4ull * nsel[2], cudaMemcpyDeviceToHost, s));
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lD.data(), d_gD, 4ull * nsel[2], cudaMemcpyDeviceToHost, s));
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lj.data(), d_gj, 4ull * nsel[2], cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lr.data(), lists[3], 4ull * nsel[3], cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lD.data(), d_gD, 4ull * nsel[3], cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lj.data(), d_gj, 4ull * nsel[3], cudaMemcpyDeviceToHost, s));
         BEEP_CUDA_TRY(cudaStreamSynchronize(s));
         st.kernel_launches += 1;
         struct R {
             uint32_t r, D, j0;
         };
-        std::vector<R> rs(nsel[2]);
-        for (uint32_t i = 0; i < nsel[2]; ++i)
+        std::vector<R> rs(nsel[3]);
+        for (uint32_t i = 0; i < nsel[3]; ++i)
             rs[i] = R{lr[i], lD[i], lj[i]};
         std::sort(rs.begin(), rs.end(), [](const R &a, const R &b) { return a.D > b.D; });
         size_t free_b = 0, total_b = 0;
@@ -898,21 +958,25 @@ beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t option
         }
         BEEP_CUDA_TRY(cudaMemsetAsync(d_cursor, 0, 16, s));
     }
-    // medium tier
-    if (nsel[1] > 0) {
-        const uint32_t maxD = max_medium;
+    // medium tiers: block per root, bitmap in shared memory
+    for (int sub = 0; sub < 2; ++sub) {
+        const uint32_t nm = nsel[1 + sub];
+        if (nm == 0)
+            continue;
+        const uint32_t maxD = sub == 0 ? max_medA : max_medB;
         const uint32_t W = (maxD + 31) / 32;
-        size_t smem = ((size_t)((maxD + 3) & ~3u) + (size_t)maxD * W) * 4;
-        int block = maxD <= 256 ? 256 : 512;
-        int per_sm = std::max(1, (int)std::min<size_t>(8, (200 * 1024) / (smem + 2048)));
-        int grid = ctx->num_sms * per_sm;
+        const size_t pad = (maxD + 4) & ~3u;
+        const size_t smem = (3 * pad + (size_t)maxD * W) * 4;
+        const int block = sub == 0 ? 256 : 1024;
+        const int per_sm = std::max(1, (int)std::min<size_t>(2048 / block, (200 * 1024) / (smem + 1024)));
+        const int grid = ctx->num_sms * per_sm;
         int tmid = tm.start();
         if (enumerate)
-            BEEP_TRY(launch_medium<true>(pl.dend, grid, block, smem, s, vd, pl, lists[1], nsel[1], rev, d_cursor + 2,
-                                         d_cnt, en, maxD));
+            BEEP_TRY(launch_medium<true>(pl.dend, grid, block, smem, s, vd, pl, lists[1 + sub], nm, rev,
+                                         d_cursor + 2 + sub, d_cnt, en, maxD));
         else
-            BEEP_TRY(launch_medium<false>(pl.dend, grid, block, smem, s, vd, pl, lists[1], nsel[1], rev,
-                                          d_cursor + 2, d_cnt, en, maxD));
+            BEEP_TRY(launch_medium<false>(pl.dend, grid, block, smem, s, vd, pl, lists[1 + sub], nm, rev,
+                                          d_cursor + 2 + sub, d_cnt, en, maxD));
         tm.stop(tmid, &st.medium_ms);
         st.medium_launches++;
         st.kernel_launches += 1;
