@@ -133,6 +133,8 @@ _SIGNATURES = [
     ("beep_count_ex", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_uint32, _P(Stats)]),
     ("beep_enumerate", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _P(ctypes.c_int32), _P(ctypes.c_uint64),
                                       _P(ctypes.c_uint64)]),
+    ("beep_count_noalloc", ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int64, _vp, _vp, _vp,
+                                          ctypes.c_int, _P(ctypes.c_uint64)]),
     ("beep_gen_erdos_renyi", ctypes.c_int, [ctypes.c_int64, ctypes.c_double, ctypes.c_uint64, _P(ctypes.c_int64),
                                             _P(ctypes.c_int64), _P(ctypes.c_int32), _P(ctypes.c_int32)]),
     ("beep_gen_rmat", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
@@ -362,6 +364,17 @@ def count(graph: Graph, query, mode: int = SGM, options: int = 0, ctx: Context |
     _check(lib().beep_count_ex(ctx.handle if ctx else None, graph.handle, q.handle, int(mode), int(options),
                                ctypes.byref(st)))
     return (int(st.count), st.as_dict()) if stats else int(st.count)
+
+
+def count_noalloc(device: int, n: int, m: int, d_row_ptr: int, d_col_ind: int, query, mode: int = SGM,
+                  cuda_stream: int | None = None) -> int:
+    """Count through the allocation-free entry point on a device CSR (sorted,
+    simple rows) given by device pointers."""
+    q = _as_query(query)
+    out = ctypes.c_uint64()
+    _check(lib().beep_count_noalloc(int(device), _vp(cuda_stream) if cuda_stream else None, int(n), int(m),
+                                    _vp(d_row_ptr), _vp(d_col_ind), q.handle, int(mode), ctypes.byref(out)))
+    return int(out.value)
 
 
 def enumerate_matches(graph: Graph, query, k: int, ctx: Context | None = None):

@@ -29,6 +29,7 @@
 //                     tasks over every warp of the GPU.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include <cub/cub.cuh>
 
@@ -1015,3 +1016,283 @@ beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t option
 }
 
 } // namespace beep
+
+// ===========================================================================
+// Allocation-free counting (beep_count_noalloc)
+//
+// Some callers cannot let a library allocate device memory: a process whose
+// device memory is handed out by its own pool or caching allocator (a
+// cudaMalloc from a library can fail there, or fragment the pool), or a
+// latency-critical loop where the device-wide synchronisation of
+// cudaMalloc/cudaFree is not acceptable. For them this path counts with no
+// allocation at all. Its only scratch is the file-scope array below, of
+// BEEP_NOALLOC_SCRATCH_BYTES: a control block (count, root cursor, largest
+// domain) and, for roots whose bitmap does not fit in shared memory, one
+// bitmap slice per block. Every GPU that loads the library holds the array
+// until the process exits. All calls on a device share it and it keeps the
+// last call's contents, so each call clears the control block first; calls
+// that overlap on the GPU (other streams or host threads) race on it.
+// ===========================================================================
+namespace beep {
+namespace {
+
+constexpr size_t kNoAllocCtrlBytes = 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BEEP_NOALLOC_SCRATCH_BYTES];
+
+struct NoAllocCtrl {
+    unsigned long long count;
+    unsigned int cursor;
+    unsigned int max_domain;
+};
+
+// Root domain straight from a sorted, simple CSR in vertex-id order.
+__device__ __forceinline__ void csr_root_domain(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
+                                                const DevPlan &pl, uint32_t r, uint32_t &beg, uint32_t &D,
+                                                uint32_t &j0, uint32_t &deg) {
+    const uint32_t b = rp[r], e = rp[r + 1];
+    const uint32_t sp = lower_bound_g(col, b, e, r) - b;
+    deg = e - b;
+    if (pl.restricted) {
+        beg = b + sp;
+        D = e - b - sp;
+        j0 = 0;
+    } else {
+        beg = b;
+        D = e - b;
+        j0 = pl.pos1_after_root ? sp : 0;
+    }
+}
+
+__device__ __forceinline__ bool csr_is_root(const DevPlan &pl, uint32_t deg, uint32_t D, uint32_t j0,
+                                            uint32_t min_deg) {
+    return deg >= min_deg && D + 1 >= (uint32_t)pl.dend && j0 < D;
+}
+
+__global__ void k_noalloc_maxdom(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n,
+                                 DevPlan pl, uint32_t min_deg, NoAllocCtrl *ctrl) {
+    uint32_t mx = 0;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t beg, D, j0, deg;
+        csr_root_domain(rp, col, pl, (uint32_t)v, beg, D, j0, deg);
+        if (csr_is_root(pl, deg, D, j0, min_deg))
+            mx = max(mx, D);
+    }
+    mx = __reduce_max_sync(kFull, mx);
+    if ((threadIdx.x & 31) == 0 && mx)
+        atomicMax(&ctrl->max_domain, mx);
+}
+
+// Rows [i0, i1) of the domain A (size D) of a root, ids ascending: the
+// higher-priority list of u is its neighbours above u.
+__device__ __forceinline__ void csr_build_rows(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
+                                               const uint32_t *A, uint32_t D, uint32_t i0, uint32_t i1,
+                                               uint32_t *rows, uint32_t W, uint32_t *s_hb, uint32_t *s_pre) {
+    const uint32_t R = i1 - i0, tid = threadIdx.x, nthr = blockDim.x;
+    for (uint32_t r = tid; r < R; r += nthr) {
+        const uint32_t i = i0 + r, u = A[i];
+        uint32_t hb = 0, c = 0;
+        if (i + 1 < D) {
+            const uint32_t b = rp[u], e = rp[u + 1];
+            const uint32_t lo = lower_bound_g(col, b, e, A[i + 1]);
+            const uint32_t hi = upper_bound_g(col, lo, e, A[D - 1]);
+            hb = lo;
+            c = hi - lo;
+        }
+        s_hb[r] = hb;
+        s_pre[r] = c;
+    }
+    __syncthreads();
+    if (tid < 32)
+        warp_excl_scan(s_pre, R, (int)tid);
+    __syncthreads();
+    const uint32_t T = s_pre[R];
+    for (uint32_t t = tid; t < T; t += nthr) {
+        uint32_t lo = 0, hi = R;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_pre[mid] <= t)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const uint32_t i = i0 + lo;
+        const uint32_t w = col[s_hb[lo] + (t - s_pre[lo])];
+        const int k = find_idx(A, i + 1, D, w);
+        if (k >= 0) {
+            atomicOr(&rows[(size_t)i * W + ((uint32_t)k >> 5)], 1u << (k & 31));
+            atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
+        }
+    }
+    __syncthreads();
+}
+
+// Block per root over every vertex (the medium-tier kernel reading the
+// caller's CSR); rows in shared memory up to smem_maxD, else in this block's
+// slice of the scratch array.
+template <int DEND>
+__global__ void __launch_bounds__(512) k_noalloc_count(const uint32_t *__restrict__ rp,
+                                                       const uint32_t *__restrict__ col, int64_t n, DevPlan pl,
+                                                       uint32_t min_deg, unsigned char *scratch,
+                                                       uint64_t slice_words, uint32_t smem_maxD) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t s_v, s_j;
+    NoAllocCtrl *ctrl = reinterpret_cast<NoAllocCtrl *>(scratch);
+    uint32_t *slice = reinterpret_cast<uint32_t *>(scratch + kNoAllocCtrlBytes) + (uint64_t)blockIdx.x * slice_words;
+    const uint32_t pad = (smem_maxD + 4) & ~3u;
+    uint32_t *sA = sm, *s_hb = sm + pad, *s_pre = sm + 2 * pad, *srows = sm + 3 * pad;
+    const int lane = threadIdx.x & 31;
+    const Lp lp = load_lp(pl);
+    EnumCtx ec{};
+    unsigned long long cnt = 0;
+    for (;;) {
+        if (threadIdx.x == 0)
+            s_v = atomicAdd(&ctrl->cursor, 1u);
+        __syncthreads();
+        const uint32_t v = s_v;
+        if ((int64_t)v >= n)
+            break;
+        uint32_t beg, D, j0, deg;
+        csr_root_domain(rp, col, pl, v, beg, D, j0, deg);
+        if (csr_is_root(pl, deg, D, j0, min_deg)) {
+            const uint32_t W = (D + 31) >> 5;
+            const bool in_smem = D <= smem_maxD;
+            uint32_t *rows = in_smem ? srows : slice;
+            const uint32_t *A = col + beg;
+            if (in_smem) {
+                for (uint32_t i = threadIdx.x; i < D; i += blockDim.x)
+                    sA[i] = A[i];
+                A = sA;
+            }
+            for (uint64_t i = threadIdx.x; i < (uint64_t)D * W; i += blockDim.x)
+                rows[i] = 0;
+            if (threadIdx.x == 0)
+                s_j = j0;
+            __syncthreads();
+            for (uint32_t i0 = 0; i0 < D; i0 += smem_maxD)
+                csr_build_rows(rp, col, A, D, i0, min(D, i0 + smem_maxD), rows, W, s_hb, s_pre);
+            for (;;) {
+                uint32_t j = 0;
+                if (lane == 0)
+                    j = atomicAdd(&s_j, 1u);
+                j = __shfl_sync(kFull, j, 0);
+                if (j >= D)
+                    break;
+                uint32_t x[kMaxQ];
+                x[1] = j;
+                dfs_warp<2, DEND, false>(lp, rows, W, D, x, cnt, lane, ec);
+            }
+        }
+        __syncthreads();
+    }
+    cnt = warp_sum(cnt);
+    if (lane == 0 && cnt)
+        atomicAdd(&ctrl->count, cnt);
+}
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[128] = {nullptr};
+
+} // namespace
+} // namespace beep
+
+extern "C" beep_status beep_count_noalloc(int device, void *cuda_stream, int64_t n, int64_t m,
+                                          const int32_t *d_row_ptr, const int32_t *d_col_ind, const beep_query *q,
+                                          beep_mode mode, uint64_t *out_count) {
+    using namespace beep;
+    if (!q || !out_count || !d_row_ptr || (m > 0 && !d_col_ind) || n < 0 || m < 0 || n >= (int64_t)0xffffffffll ||
+        m >= (int64_t)0xffffffffll)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_count_noalloc: bad arguments");
+    if (device < 0 || device >= 128)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_count_noalloc: device id out of range");
+    if (mode != BEEP_MODE_SGM && mode != BEEP_MODE_SGC)
+        return fail(BEEP_ERR_INVALID_ARG, "unknown mode");
+    BEEP_CUDA_TRY(cudaSetDevice(device));
+    // Set-up, once per device with the device current: the device address of
+    // the scratch array (its host-side name is not a device address).
+    void *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[device]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p)
+                return fail(BEEP_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+            g_noalloc_ptr[device] = p;
+        }
+        scratch = g_noalloc_ptr[device];
+    }
+    QueryPlan plan;
+    BEEP_TRY(compile_plan(q->impl.qn, q->impl.row_ptr, q->impl.col, mode, &plan));
+    if (plan.dev.dend < 3) {
+        *out_count = 0;
+        return BEEP_OK;
+    }
+    if (mode == BEEP_MODE_SGC && plan.info.unmat)
+        return fail(BEEP_ERR_UNSUPPORTED, "sgc with an unmaterialised last level depends on the reference's priority "
+                                          "order, which needs the peeled and relabelled graph: use beep_count");
+    DevPlan pl = plan.dev;
+    pl.asc = 1; // vertex ids ascending are the priority order here
+    cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+    const uint32_t *rp = reinterpret_cast<const uint32_t *>(d_row_ptr);
+    const uint32_t *col = reinterpret_cast<const uint32_t *>(d_col_ind);
+    NoAllocCtrl *ctrl = reinterpret_cast<NoAllocCtrl *>(scratch);
+    int num_sms = 148;
+    BEEP_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    BEEP_CUDA_TRY(cudaMemsetAsync(scratch, 0, kNoAllocCtrlBytes, s));
+    const uint32_t min_deg = (uint32_t)plan.info.max_qdeg;
+    if (n > 0) {
+        const int g0 = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms * 16));
+        k_noalloc_maxdom<<<g0, 256, 0, s>>>(rp, col, n, pl, min_deg, ctrl);
+        BEEP_CUDA_TRY(cudaGetLastError());
+    }
+    uint32_t maxD = 0;
+    BEEP_CUDA_TRY(cudaMemcpyAsync(&maxD, &ctrl->max_domain, sizeof(maxD), cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (maxD == 0) {
+        *out_count = 0;
+        return BEEP_OK;
+    }
+    const uint32_t smem_maxD = (uint32_t)kMediumMaxD;
+    const uint64_t arena_words = (BEEP_NOALLOC_SCRATCH_BYTES - kNoAllocCtrlBytes) / 4;
+    uint64_t slice_words = 0;
+    int grid = num_sms;
+    if (maxD > smem_maxD) {
+        slice_words = ((uint64_t)maxD * ((maxD + 31) / 32) + 63) & ~(uint64_t)63;
+        if (slice_words > arena_words)
+            return fail(BEEP_ERR_UNSUPPORTED,
+                        "beep_count_noalloc: the largest search domain has " + std::to_string(maxD) +
+                            " vertices; its bitmap needs " + std::to_string(slice_words * 4) +
+                            " bytes, more than the " + std::to_string(BEEP_NOALLOC_SCRATCH_BYTES) +
+                            "-byte scratch of the allocation-free path (domains up to 23170 vertices); use beep_count");
+        grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms, arena_words / slice_words));
+    }
+    const size_t pad = (smem_maxD + 4) & ~3u;
+    const size_t smem = (3 * pad + (size_t)smem_maxD * ((smem_maxD + 31) / 32)) * 4;
+    unsigned char *scr = static_cast<unsigned char *>(scratch);
+    switch (pl.dend) {
+#define BEEP_CASE(DD)                                                                                              \
+    case DD:                                                                                                       \
+        BEEP_CUDA_TRY(cudaFuncSetAttribute(k_noalloc_count<DD>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                           (int)smem));                                                            \
+        k_noalloc_count<DD><<<grid, 512, smem, s>>>(rp, col, n, pl, min_deg, scr, slice_words, smem_maxD);          \
+        break;
+        BEEP_CASE(3)
+        BEEP_CASE(4)
+        BEEP_CASE(5)
+        BEEP_CASE(6)
+        BEEP_CASE(7)
+        BEEP_CASE(8)
+        BEEP_CASE(9)
+        BEEP_CASE(10)
+#undef BEEP_CASE
+    default:
+        return fail(BEEP_ERR_UNSUPPORTED, "depth out of range");
+    }
+    BEEP_CUDA_TRY(cudaGetLastError());
+    unsigned long long c = 0;
+    BEEP_CUDA_TRY(cudaMemcpyAsync(&c, &ctrl->count, sizeof(c), cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    *out_count = c;
+    return BEEP_OK;
+}

@@ -190,6 +190,42 @@ beep_status beep_count_ex(beep_ctx *ctx, beep_graph *g, const beep_query *q, bee
 beep_status beep_enumerate(beep_ctx *ctx, beep_graph *g, const beep_query *q, uint64_t k, int32_t *out_tuples,
                            uint64_t *n_out, uint64_t *total_count);
 
+/* ---- counting without allocation --------------------------------------- */
+
+/* Size of the device scratch array the allocation-free path uses (64 MiB per
+ * device, held from the first call until the process exits). */
+#define BEEP_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* Count matches without allocating any device memory. No counterpart in the
+ * reference: it exists for callers that cannot let a library call cudaMalloc
+ * -- processes whose device memory belongs to their own pool or caching
+ * allocator (a library allocation can fail there or fragment the pool) and
+ * latency-critical loops that cannot afford the device-wide synchronisation
+ * of cudaMalloc/cudaFree.
+ *
+ * Input: the caller's CSR in device memory on `device` (rows sorted
+ * ascending, no duplicate edge, no self loop, both directions -- the form
+ * beep_graph_csr returns); output: the count written to *out_count (host).
+ * Work is ordered on cuda_stream (NULL: the legacy default stream) and the
+ * call returns when it is done. It calls no cudaMalloc, cudaFree or other
+ * allocating routine: its only scratch is a file-scope device array of
+ * BEEP_NOALLOC_SCRATCH_BYTES. The first call on a device looks up that array's
+ * device address; make that first call before any stream capture.
+ *
+ * The graph is neither peeled nor relabelled: vertex ids give the symmetry-
+ * breaking order, which leaves sgm counts unchanged. sgc queries whose last
+ * level is unmaterialised (LUNMAT = 1) depend on the reference's degree order
+ * and are refused with BEEP_ERR_UNSUPPORTED. Roots whose search domain exceeds
+ * 1024 vertices keep their bitmap in the scratch array, so the largest domain
+ * (a root's neighbours, or its higher-id neighbours for clique-like queries)
+ * is limited to 23170 vertices; larger inputs are refused with
+ * BEEP_ERR_UNSUPPORTED before any work. The fewer such slices fit, the fewer
+ * blocks run. All calls on a device share the scratch array, which keeps the
+ * last call's contents (each call clears what must start at zero); calls that
+ * overlap on the GPU, from other streams or host threads, race on it. */
+beep_status beep_count_noalloc(int device, void *cuda_stream, int64_t n, int64_t m, const int32_t *d_row_ptr,
+                               const int32_t *d_col_ind, const beep_query *q, beep_mode mode, uint64_t *out_count);
+
 /* ---- synthetic inputs and files ---------------------------------------- */
 
 /* Deterministic generators (splitmix64 streams keyed by seed and edge index).
