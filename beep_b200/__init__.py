@@ -35,6 +35,7 @@ OPT_REFERENCE_ROOT_CAP = 1 << 0
 OPT_TIMING = 1 << 1
 OPT_NO_VIEW_CACHE = 1 << 2
 OPT_ALG_BYTES = 1 << 3
+OPT_NO_GRAPH = 1 << 4
 
 
 class BeepError(RuntimeError):
@@ -133,6 +134,11 @@ _SIGNATURES = [
     ("beep_count_ex", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_uint32, _P(Stats)]),
     ("beep_enumerate", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _P(ctypes.c_int32), _P(ctypes.c_uint64),
                                       _P(ctypes.c_uint64)]),
+    ("beep_batch_create", ctypes.c_int, [_vp, _P(_vp)]),
+    ("beep_batch_add", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _P(ctypes.c_uint32)]),
+    ("beep_batch_run", ctypes.c_int, [_vp, ctypes.c_uint32, _P(ctypes.c_uint64), _P(Stats)]),
+    ("beep_batch_size", ctypes.c_int, [_vp, _P(ctypes.c_uint32)]),
+    ("beep_batch_destroy", ctypes.c_int, [_vp]),
     ("beep_count_noalloc", ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int64, _vp, _vp, _vp,
                                           ctypes.c_int, _P(ctypes.c_uint64)]),
     ("beep_gen_erdos_renyi", ctypes.c_int, [ctypes.c_int64, ctypes.c_double, ctypes.c_uint64, _P(ctypes.c_int64),
@@ -364,6 +370,49 @@ def count(graph: Graph, query, mode: int = SGM, options: int = 0, ctx: Context |
     _check(lib().beep_count_ex(ctx.handle if ctx else None, graph.handle, q.handle, int(mode), int(options),
                                ctypes.byref(st)))
     return (int(st.count), st.as_dict()) if stats else int(st.count)
+
+
+class Batch:
+    """Many (graph, query, mode) pairs counted by one set of launches,
+    captured into a CUDA graph on the first run and replayed afterwards."""
+
+    def __init__(self, ctx: Context):
+        h = _vp()
+        _check(lib().beep_batch_create(ctx.handle, ctypes.byref(h)))
+        self._h = h
+        self.ctx = ctx
+        self._keep = []  # graphs and queries must outlive the batch
+
+    def add(self, graph: Graph, query, mode: int = SGM) -> int:
+        q = _as_query(query)
+        idx = ctypes.c_uint32()
+        _check(lib().beep_batch_add(self._h, graph.handle, q.handle, int(mode), ctypes.byref(idx)))
+        self._keep.append((graph, q))
+        return int(idx.value)
+
+    def __len__(self) -> int:
+        n = ctypes.c_uint32()
+        _check(lib().beep_batch_size(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def run(self, options: int = 0, stats: bool = False):
+        n = len(self)
+        counts = (ctypes.c_uint64 * max(n, 1))()
+        st = Stats()
+        _check(lib().beep_batch_run(self._h, int(options), counts, ctypes.byref(st)))
+        out = [int(counts[i]) for i in range(n)]
+        return (out, st.as_dict()) if stats else out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().beep_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def count_noalloc(device: int, n: int, m: int, d_row_ptr: int, d_col_ind: int, query, mode: int = SGM,

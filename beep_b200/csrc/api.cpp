@@ -105,6 +105,19 @@ beep_status beep_ctx_create(int device, void *stream, beep_ctx **out) {
     }
     if (e == cudaSuccess)
         e = cudaMallocHost(&c->impl.h_pinned, 64);
+    if (e == cudaSuccess) {
+        // per-call buffers come from a pool of this context that keeps its memory
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        e = cudaMemPoolCreate(&c->impl.pool, &props);
+        if (e == cudaSuccess) {
+            uint64_t keep = ~0ull;
+            e = cudaMemPoolSetAttribute(c->impl.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (e != cudaSuccess) {
         delete c;
         return fail(BEEP_ERR_CUDA, std::string("context setup: ") + cudaGetErrorString(e));
@@ -123,6 +136,10 @@ void ctx_free(beep_ctx *ctx) {
     ctx->impl.counter.release();
     if (ctx->impl.h_pinned)
         cudaFreeHost(ctx->impl.h_pinned);
+    if (ctx->impl.h_results)
+        cudaFreeHost(ctx->impl.h_results);
+    if (ctx->impl.pool)
+        cudaMemPoolDestroy(ctx->impl.pool);
     if (ctx->impl.own_stream)
         cudaStreamDestroy(ctx->impl.stream);
     delete ctx;
@@ -369,6 +386,93 @@ beep_status beep_enumerate(beep_ctx *ctx, beep_graph *g, const beep_query *q, ui
     *n_out = got;
     if (total_count)
         *total_count = st.count;
+    return BEEP_OK;
+}
+
+struct beep_batch {
+    beep_ctx *ctx = nullptr;
+    std::vector<beep::PairSpec> specs;
+    beep::LaunchPlanPtr plan;
+    uint32_t planned_options = 0;
+};
+
+beep_status beep_batch_create(beep_ctx *ctx, beep_batch **out) {
+    if (!ctx || !out)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_batch_create: bad arguments");
+    auto *b = new beep_batch;
+    b->ctx = ctx;
+    ctx->refs.fetch_add(1);
+    *out = b;
+    return BEEP_OK;
+}
+
+beep_status beep_batch_add(beep_batch *b, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t *index) {
+    if (!b || !g || !q)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_batch_add: bad arguments");
+    if (mode != BEEP_MODE_SGM && mode != BEEP_MODE_SGC)
+        return fail(BEEP_ERR_INVALID_ARG, "unknown mode");
+    if (g->impl.device != b->ctx->impl.device)
+        return fail(BEEP_ERR_INVALID_ARG, "graph lives on another device");
+    PairSpec ps;
+    ps.g = &g->impl;
+    BEEP_TRY(compile_plan(q->impl.qn, q->impl.row_ptr, q->impl.col, mode, &ps.plan));
+    b->specs.push_back(ps);
+    b->plan.reset(); // re-plan on the next run
+    if (index)
+        *index = (uint32_t)(b->specs.size() - 1);
+    return BEEP_OK;
+}
+
+beep_status beep_batch_size(const beep_batch *b, uint32_t *out) {
+    if (!b || !out)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_batch_size: bad arguments");
+    *out = (uint32_t)b->specs.size();
+    return BEEP_OK;
+}
+
+beep_status beep_batch_run(beep_batch *b, uint32_t options, uint64_t *counts, beep_stats *stats) {
+    if (!b || (!counts && !b->specs.empty()))
+        return fail(BEEP_ERR_INVALID_ARG, "beep_batch_run: bad arguments");
+    BEEP_TRY(bind(b->ctx));
+    Ctx *ctx = &b->ctx->impl;
+    const uint32_t plan_opts = options & (BEEP_OPT_REFERENCE_ROOT_CAP | BEEP_OPT_NO_VIEW_CACHE);
+    double prep_ms = 0;
+    if (!b->plan || b->planned_options != plan_opts) {
+        b->plan.reset();
+        cudaEvent_t p0, p1;
+        cudaEventCreate(&p0);
+        cudaEventCreate(&p1);
+        cudaEventRecord(p0, ctx->stream);
+        BEEP_TRY(plan_pairs(ctx, b->specs, plan_opts, &b->plan));
+        b->planned_options = plan_opts;
+        cudaEventRecord(p1, ctx->stream);
+        cudaEventSynchronize(p1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p0, p1);
+        prep_ms = ms;
+        cudaEventDestroy(p0);
+        cudaEventDestroy(p1);
+    }
+    if (!(options & BEEP_OPT_NO_GRAPH) && !(options & BEEP_OPT_TIMING))
+        BEEP_TRY(capture_plan(ctx, b->plan.get()));
+    beep_stats st;
+    BEEP_TRY(execute_plan(ctx, b->plan.get(), options, &b->specs, counts, b->specs.size(), &st));
+    st.prep_ms = prep_ms;
+    ctx->launches += (uint64_t)st.kernel_launches;
+    if (stats)
+        *stats = st;
+    return BEEP_OK;
+}
+
+beep_status beep_batch_destroy(beep_batch *b) {
+    if (!b)
+        return BEEP_OK;
+    beep_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->impl.device);
+    b->plan.reset();
+    cudaStreamSynchronize(ctx->impl.stream);
+    delete b;
+    ctx_release(ctx);
     return BEEP_OK;
 }
 

@@ -360,36 +360,97 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
 }
 
 // ---------------------------------------------------------------------------
-// small tier: warp per root
+// work items. A pair is one (graph view, compiled query); an item is one root
+// of one pair, packed as (pair << 32) | root. One launch per tier serves the
+// items of every pair of a call (the plain count is a call with one pair).
+// ---------------------------------------------------------------------------
+struct PairDev {
+    ViewDev v;
+    DevPlan pl;
+    unsigned long long *count; // this pair's match count
+    EnumDev en;                // enumeration output (out == nullptr: none)
+    uint32_t min_deg;          // roots: degree >= max_qdeg ...
+    uint32_t cap_deg;          // ... and < cap_deg (reference root cap, else 2^32-1)
+};
+
+__device__ __forceinline__ uint32_t item_pair(uint64_t it) { return (uint32_t)(it >> 32); }
+__device__ __forceinline__ uint32_t item_root(uint64_t it) { return (uint32_t)it; }
+
+// The fields of a pair a kernel keeps in registers while it works on the
+// pair's items (items are grouped by pair, so it reloads rarely).
+struct PairRegs {
+    ViewDev v;
+    Lp lp;
+    int restricted, pos1, asc;
+    unsigned long long *count;
+};
+
+__device__ __forceinline__ void load_pair(const PairDev *__restrict__ pairs, uint32_t p, PairRegs &pr) {
+    const PairDev &pd = pairs[p];
+    pr.v = pd.v;
+    pr.lp = load_lp(pd.pl);
+    pr.restricted = pd.pl.restricted;
+    pr.pos1 = pd.pl.pos1_after_root;
+    pr.asc = pd.pl.asc;
+    pr.count = pd.count;
+}
+
+__device__ __forceinline__ void pair_domain(const PairRegs &pr, uint32_t r, uint32_t &beg, uint32_t &D,
+                                            uint32_t &j0) {
+    const uint32_t b = pr.v.rp[r], e = pr.v.rp[r + 1], sp = pr.v.split[r];
+    if (pr.restricted) {
+        beg = b + sp;
+        D = e - b - sp;
+        j0 = 0;
+    } else {
+        beg = b;
+        D = e - b;
+        // position 1 symmetric to the root: only neighbours after the root
+        // (sgm_kernelsLD.cuh:60)
+        j0 = pr.pos1 ? sp : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// small tier: warp per root, 64-bit rows, one lane per level-1 vertex
 // ---------------------------------------------------------------------------
 constexpr int kSmallWarps = 8;
 
 template <int DEND, bool ENUM>
-__global__ void __launch_bounds__(kSmallWarps * 32) k_small(ViewDev v, DevPlan pl, const uint32_t *__restrict__ roots,
-                                                           uint32_t nroots, int rev, unsigned long long *counter,
-                                                           EnumDev en) {
+__global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__restrict__ pairs,
+                                                           const uint64_t *__restrict__ items, uint32_t nitems) {
     __shared__ uint64_t s_rows[kSmallWarps][kSmallMaxD];
     __shared__ uint32_t s_A[kSmallWarps][kSmallMaxD];
     __shared__ uint32_t s_hb[kSmallWarps][kSmallMaxD];
     __shared__ uint32_t s_pre[kSmallWarps][kSmallMaxD + 1];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const Lp lp = load_lp(pl);
     uint64_t *rows = s_rows[wib];
     uint32_t *A = s_A[wib];
+    PairRegs pr;
+    uint32_t cur = 0xffffffffu;
     EnumCtx ec;
-    if constexpr (ENUM)
-        make_ec(ec, en, pl, v);
     unsigned long long cnt = 0;
-    for (uint32_t ri = blockIdx.x * kSmallWarps + wib; ri < nroots; ri += gridDim.x * kSmallWarps) {
-        const uint32_t r = roots[rev ? nroots - 1 - ri : ri];
+    for (uint32_t ri = blockIdx.x * kSmallWarps + wib; ri < nitems; ri += gridDim.x * kSmallWarps) {
+        const uint64_t it = items[ri];
+        const uint32_t p = item_pair(it), r = item_root(it);
+        if (p != cur) { // warp-uniform
+            cnt = warp_sum(cnt);
+            if (lane == 0 && cnt)
+                atomicAdd(pr.count, cnt);
+            cnt = 0;
+            cur = p;
+            load_pair(pairs, p, pr);
+            if constexpr (ENUM)
+                make_ec(ec, pairs[p].en, pairs[p].pl, pr.v);
+        }
         uint32_t beg, D, j0;
-        root_domain(v, pl, r, beg, D, j0);
+        pair_domain(pr, r, beg, D, j0);
         for (uint32_t i = lane; i < D; i += 32) {
-            A[i] = v.col[beg + i];
+            A[i] = pr.v.col[beg + i];
             rows[i] = 0;
         }
         __syncwarp();
-        build_rows_flat<false>(v, pl.asc, A, D, 0, D, s_hb[wib], s_pre[wib], (uint32_t)lane, 32u,
+        build_rows_flat<false>(pr.v, pr.asc, A, D, 0, D, s_hb[wib], s_pre[wib], (uint32_t)lane, 32u,
                                [&](uint32_t i, uint32_t k) {
                                    atomicOr((unsigned long long *)&rows[i], 1ull << k);
                                    atomicOr((unsigned long long *)&rows[k], 1ull << i);
@@ -403,54 +464,64 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(ViewDev v, DevPlan p
         for (uint32_t j = j0 + lane; j < D; j += 32) {
             uint32_t x[kMaxQ];
             x[1] = j;
-            dfs_thread<2, DEND, ENUM>(lp, rows, all, x, cnt, ec);
+            dfs_thread<2, DEND, ENUM>(pr.lp, rows, all, x, cnt, ec);
         }
         __syncwarp();
     }
     cnt = warp_sum(cnt);
     if (lane == 0 && cnt)
-        atomicAdd(counter, cnt);
+        atomicAdd(pr.count, cnt);
 }
 
 // ---------------------------------------------------------------------------
 // medium tier: block per root, bitmap in shared memory
 // ---------------------------------------------------------------------------
 template <int DEND, bool ENUM>
-__global__ void __launch_bounds__(1024) k_medium(ViewDev v, DevPlan pl, const uint32_t *__restrict__ roots,
-                                                uint32_t nroots, int rev, unsigned *cursor,
-                                                unsigned long long *counter, EnumDev en, uint32_t maxD) {
+__global__ void __launch_bounds__(1024) k_medium(const PairDev *__restrict__ pairs,
+                                                const uint64_t *__restrict__ items, uint32_t nitems,
+                                                unsigned *cursor, uint32_t maxD) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t s_ri, s_j;
     const int lane = threadIdx.x & 31;
-    const Lp lp = load_lp(pl);
     const uint32_t pad = (maxD + 4) & ~3u;
     uint32_t *A = sm;
     uint32_t *s_hb = sm + pad;
     uint32_t *s_pre = sm + 2 * pad;
     uint32_t *rows = sm + 3 * pad;
+    PairRegs pr;
+    uint32_t cur = 0xffffffffu;
     EnumCtx ec;
-    if constexpr (ENUM)
-        make_ec(ec, en, pl, v);
     unsigned long long cnt = 0;
     for (;;) {
         if (threadIdx.x == 0)
             s_ri = atomicAdd(cursor, 1u);
         __syncthreads();
         const uint32_t ri = s_ri;
-        if (ri >= nroots)
+        if (ri >= nitems)
             break;
-        const uint32_t r = roots[rev ? nroots - 1 - ri : ri];
+        const uint64_t it = items[ri];
+        const uint32_t p = item_pair(it), r = item_root(it);
+        if (p != cur) { // block-uniform
+            cnt = warp_sum(cnt);
+            if (lane == 0 && cnt)
+                atomicAdd(pr.count, cnt);
+            cnt = 0;
+            cur = p;
+            load_pair(pairs, p, pr);
+            if constexpr (ENUM)
+                make_ec(ec, pairs[p].en, pairs[p].pl, pr.v);
+        }
         uint32_t beg, D, j0;
-        root_domain(v, pl, r, beg, D, j0);
+        pair_domain(pr, r, beg, D, j0);
         const uint32_t W = (D + 31) >> 5;
         for (uint32_t i = threadIdx.x; i < D; i += blockDim.x)
-            A[i] = v.col[beg + i];
+            A[i] = pr.v.col[beg + i];
         for (uint32_t i = threadIdx.x; i < D * W; i += blockDim.x)
             rows[i] = 0;
         if (threadIdx.x == 0)
             s_j = j0;
         __syncthreads();
-        build_rows_flat<true>(v, pl.asc, A, D, 0, D, s_hb, s_pre, threadIdx.x, blockDim.x,
+        build_rows_flat<true>(pr.v, pr.asc, A, D, 0, D, s_hb, s_pre, threadIdx.x, blockDim.x,
                               [&](uint32_t i, uint32_t k) {
                                   atomicOr(&rows[(size_t)i * W + (k >> 5)], 1u << (k & 31));
                                   atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
@@ -469,20 +540,20 @@ __global__ void __launch_bounds__(1024) k_medium(ViewDev v, DevPlan pl, const ui
                 break;
             uint32_t x[kMaxQ];
             x[1] = j;
-            dfs_warp<2, DEND, ENUM>(lp, rows, W, D, x, cnt, lane, ec);
+            dfs_warp<2, DEND, ENUM>(pr.lp, rows, W, D, x, cnt, lane, ec);
         }
         __syncthreads();
     }
     cnt = warp_sum(cnt);
     if (lane == 0 && cnt)
-        atomicAdd(counter, cnt);
+        atomicAdd(pr.count, cnt);
 }
 
 // ---------------------------------------------------------------------------
 // large tier: rows of a batch of roots in a global arena
 // ---------------------------------------------------------------------------
 struct Batch {
-    const uint32_t *root;    // [nb]
+    const uint64_t *item;    // [nb] (pair, root)
     const uint64_t *off;     // [nb] word offset of the root's rows in the arena
     const uint32_t *cstart;  // [nb+1] prefix of row chunks
     const uint32_t *tstart;  // [nb+1] prefix of DFS tasks (level-1 vertices)
@@ -505,7 +576,7 @@ __device__ __forceinline__ uint32_t find_batch(const uint32_t *__restrict__ star
     return lo;
 }
 
-__global__ void __launch_bounds__(512) k_large_rows(ViewDev v, DevPlan pl, Batch bt, uint32_t *arena,
+__global__ void __launch_bounds__(512) k_large_rows(const PairDev *__restrict__ pairs, Batch bt, uint32_t *arena,
                                                     unsigned *cursor) {
     extern __shared__ __align__(16) uint32_t sA[];
     __shared__ uint32_t s_c;
@@ -519,21 +590,23 @@ __global__ void __launch_bounds__(512) k_large_rows(ViewDev v, DevPlan pl, Batch
         if (c >= total)
             break;
         const uint32_t b = find_batch(bt.cstart, bt.nb, c);
-        const uint32_t r = bt.root[b];
+        const uint64_t it = bt.item[b];
+        PairRegs pr;
+        load_pair(pairs, item_pair(it), pr);
         uint32_t beg, D, j0;
-        root_domain(v, pl, r, beg, D, j0);
+        pair_domain(pr, item_root(it), beg, D, j0);
         const uint32_t W = (D + 31) >> 5;
         uint32_t *rows = arena + bt.off[b];
         const uint32_t i0 = (c - bt.cstart[b]) * kRowsPerChunk;
         const uint32_t i1 = min(D, i0 + kRowsPerChunk);
-        const uint32_t *A = v.col + beg;
+        const uint32_t *A = pr.v.col + beg;
         if (D <= kLargeSmemA) {
             for (uint32_t i = threadIdx.x; i < D; i += blockDim.x)
                 sA[i] = A[i];
             __syncthreads();
             A = sA;
         }
-        build_rows_flat<true>(v, pl.asc, A, D, i0, i1, s_hb, s_pre, threadIdx.x, blockDim.x,
+        build_rows_flat<true>(pr.v, pr.asc, A, D, i0, i1, s_hb, s_pre, threadIdx.x, blockDim.x,
                               [&](uint32_t i, uint32_t k) {
                                   atomicOr(&rows[(size_t)i * W + (k >> 5)], 1u << (k & 31));
                                   atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
@@ -543,14 +616,13 @@ __global__ void __launch_bounds__(512) k_large_rows(ViewDev v, DevPlan pl, Batch
 }
 
 template <int DEND, bool ENUM>
-__global__ void __launch_bounds__(256) k_large_dfs(ViewDev v, DevPlan pl, Batch bt, const uint32_t *arena,
-                                                   unsigned *cursor, unsigned long long *counter, EnumDev en) {
+__global__ void __launch_bounds__(256) k_large_dfs(const PairDev *__restrict__ pairs, Batch bt,
+                                                   const uint32_t *arena, unsigned *cursor) {
     const int lane = threadIdx.x & 31;
-    const Lp lp = load_lp(pl);
     const uint32_t total = bt.tstart[bt.nb];
+    PairRegs pr;
+    uint32_t cur = 0xffffffffu;
     EnumCtx ec;
-    if constexpr (ENUM)
-        make_ec(ec, en, pl, v);
     unsigned long long cnt = 0;
     for (;;) {
         uint32_t t = 0;
@@ -560,60 +632,122 @@ __global__ void __launch_bounds__(256) k_large_dfs(ViewDev v, DevPlan pl, Batch 
         if (t >= total)
             break;
         const uint32_t b = find_batch(bt.tstart, bt.nb, t);
-        const uint32_t r = bt.root[b];
+        const uint64_t it = bt.item[b];
+        const uint32_t p = item_pair(it), r = item_root(it);
+        if (p != cur) {
+            cnt = warp_sum(cnt);
+            if (lane == 0 && cnt)
+                atomicAdd(pr.count, cnt);
+            cnt = 0;
+            cur = p;
+            load_pair(pairs, p, pr);
+            if constexpr (ENUM)
+                make_ec(ec, pairs[p].en, pairs[p].pl, pr.v);
+        }
         uint32_t beg, D, j0;
-        root_domain(v, pl, r, beg, D, j0);
+        pair_domain(pr, r, beg, D, j0);
         const uint32_t W = (D + 31) >> 5;
         if constexpr (ENUM) {
-            ec.A = v.col + beg;
+            ec.A = pr.v.col + beg;
             ec.root = r;
         }
         uint32_t x[kMaxQ];
         x[1] = j0 + (t - bt.tstart[b]);
-        dfs_warp<2, DEND, ENUM>(lp, arena + bt.off[b], W, D, x, cnt, lane, ec);
+        dfs_warp<2, DEND, ENUM>(pr.lp, arena + bt.off[b], W, D, x, cnt, lane, ec);
     }
     cnt = warp_sum(cnt);
     if (lane == 0 && cnt)
-        atomicAdd(counter, cnt);
+        atomicAdd(pr.count, cnt);
 }
 
 // ---------------------------------------------------------------------------
-// root classification
+// root classification over the vertices of every pair (flattened index)
 // ---------------------------------------------------------------------------
-// tier: 0 none, 1 small, 2 medium (D <= 256), 3 medium (D <= 1024), 4 large. Also accumulates the adjacency
-// bytes the kernels must read for the roofline.
-__global__ void k_classify(ViewDev v, DevPlan pl, int64_t n, uint32_t min_deg, uint32_t cap_deg, uint8_t *tier,
-                           uint32_t *dom, unsigned *tier_max) {
-    uint32_t mx[4] = {0, 0, 0, 0};
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t deg = v.rp[r + 1] - v.rp[r];
-        uint32_t beg, D, j0;
-        root_domain(v, pl, (uint32_t)r, beg, D, j0);
-        uint8_t t = 0;
-        // roots: degree in [max_qdeg, cap) (subgraph_matching.cuh:1086-1098);
+constexpr int kTiers = 4;   // 1 small (D <= 64), 2 medium (<= 256), 3 medium (<= 1024), 4 large
+constexpr int kDepths = 11; // dend 0..10
+
+__device__ __forceinline__ uint32_t find_pair(const uint64_t *__restrict__ offs, uint32_t npairs, uint64_t t) {
+    uint32_t lo = 0, hi = npairs;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (offs[mid] <= t)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// tier[t] for flattened vertex t; dom[t] = its domain size; per tier the
+// largest domain and per (tier, depth) the number of roots.
+__global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ offs, uint32_t npairs,
+                           uint64_t N, uint8_t *tier, uint32_t *dom, unsigned *tier_max, unsigned *tier_depth) {
+    __shared__ unsigned s_hist[kTiers * kDepths];
+    for (int i = threadIdx.x; i < kTiers * kDepths; i += blockDim.x)
+        s_hist[i] = 0;
+    __syncthreads();
+    uint32_t mx[kTiers] = {0, 0, 0, 0};
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = find_pair(offs, npairs, t);
+        const uint32_t r = (uint32_t)(t - offs[p]);
+        const PairDev &pd = pairs[p];
+        const uint32_t deg = pd.v.rp[r + 1] - pd.v.rp[r];
+        const uint32_t sp = pd.v.split[r];
+        uint32_t D, j0;
+        if (pd.pl.restricted) {
+            D = deg - sp;
+            j0 = 0;
+        } else {
+            D = deg;
+            j0 = pd.pl.pos1_after_root ? sp : 0;
+        }
+        uint8_t tc = 0;
+        // roots: degree in [max_qdeg, cap) (subgraph_matching.cuh:1086-1098),
         // enough domain vertices for the other dend-1 positions and at least
-        // one level-1 vertex.
-        if (deg >= min_deg && deg < cap_deg && D + 1 >= (uint32_t)pl.dend && j0 < D)
-            t = D <= kSmallMaxD ? 1 : (D <= kMediumAMaxD ? 2 : (D <= kMediumMaxD ? 3 : 4));
-        tier[r] = t;
-        dom[r] = D;
-        if (t)
-            mx[t - 1] = max(mx[t - 1], D);
+        // one level-1 vertex
+        if (deg >= pd.min_deg && deg < pd.cap_deg && D + 1 >= (uint32_t)pd.pl.dend && j0 < D)
+            tc = D <= kSmallMaxD ? 1 : (D <= kMediumAMaxD ? 2 : (D <= kMediumMaxD ? 3 : 4));
+        tier[t] = tc;
+        dom[t] = D;
+        if (tc) {
+            mx[tc - 1] = max(mx[tc - 1], D);
+            atomicAdd(&s_hist[(tc - 1) * kDepths + pd.pl.dend], 1u);
+        }
     }
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const uint32_t m = __reduce_max_sync(kFull, mx[t]);
+    for (int k = 0; k < kTiers; ++k) {
+        const uint32_t m = __reduce_max_sync(kFull, mx[k]);
         if ((threadIdx.x & 31) == 0 && m)
-            atomicMax(&tier_max[t], m);
+            atomicMax(&tier_max[k], m);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kTiers * kDepths; i += blockDim.x)
+        if (s_hist[i])
+            atomicAdd(&tier_depth[i], s_hist[i]);
+}
+
+// Selected flattened indices -> items and sort keys: depth, then (medium)
+// largest domain first.
+__global__ void k_make_items(const uint32_t *__restrict__ sel, uint32_t ns, const PairDev *__restrict__ pairs,
+                             const uint64_t *__restrict__ offs, uint32_t npairs, const uint32_t *__restrict__ dom,
+                             int by_domain, uint64_t *items, uint32_t *keys) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
+        const uint32_t t = sel[i];
+        const uint32_t p = find_pair(offs, npairs, t);
+        items[i] = ((uint64_t)p << 32) | (uint64_t)(t - offs[p]);
+        const uint32_t dend = (uint32_t)pairs[p].pl.dend;
+        keys[i] = by_domain ? (dend << 16) | (65535u - min(dom[t], 65535u)) : dend;
     }
 }
 
-// (D, j0) of each listed root.
-__global__ void k_gather_dom(ViewDev v, DevPlan pl, const uint32_t *__restrict__ list, uint32_t nl, uint32_t *D_out,
-                             uint32_t *j0_out) {
+// (D, j0) of each listed item.
+__global__ void k_gather_dom(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ items, uint32_t nl,
+                             uint32_t *D_out, uint32_t *j0_out) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nl; i += gridDim.x * blockDim.x) {
+        PairRegs pr;
+        load_pair(pairs, item_pair(items[i]), pr);
         uint32_t beg, D, j0;
-        root_domain(v, pl, list[i], beg, D, j0);
+        pair_domain(pr, item_root(items[i]), beg, D, j0);
         D_out[i] = D;
         j0_out[i] = j0;
     }
@@ -622,30 +756,33 @@ __global__ void k_gather_dom(ViewDev v, DevPlan pl, const uint32_t *__restrict__
 // Adjacency bytes of the searched roots: row pointers and split of the root
 // (12 B), its domain list (4 B each) and, per domain vertex, its row pointers
 // and split (12 B) plus its higher-priority list (4 B each).
-__global__ void k_alg_bytes(ViewDev v, DevPlan pl, const uint8_t *__restrict__ tier, int64_t n,
-                            unsigned long long *bytes) {
+__global__ void k_alg_bytes(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ offs, uint32_t npairs,
+                            const uint8_t *__restrict__ tier, uint64_t N, unsigned long long *bytes) {
     unsigned long long acc[3] = {0, 0, 0};
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
-        const int t = tier[r];
-        if (!t)
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < N; t += warps) {
+        const int tc = tier[t];
+        if (!tc)
             continue;
+        const uint32_t p = find_pair(offs, npairs, t);
+        PairRegs pr;
+        load_pair(pairs, p, pr);
         uint32_t beg, D, j0;
-        root_domain(v, pl, (uint32_t)r, beg, D, j0);
+        pair_domain(pr, (uint32_t)(t - offs[p]), beg, D, j0);
         unsigned long long a = (lane == 0) ? 12ull + 4ull * D : 0ull;
         for (uint32_t i = lane; i < D; i += 32) {
             uint32_t hb, he, xb, xe;
-            hd_range(v, pl.asc, v.col[beg + i], i, D, hb, he, xb, xe);
+            hd_range(pr.v, pr.asc, pr.v.col[beg + i], i, D, hb, he, xb, xe);
             a += 12ull + 4ull * (he - hb);
         }
-        acc[t == 1 ? 0 : (t == 4 ? 2 : 1)] += a;
+        acc[tc == 1 ? 0 : (tc == 4 ? 2 : 1)] += a;
     }
 #pragma unroll
-    for (int t = 0; t < 3; ++t) {
-        const unsigned long long x = warp_sum(acc[t]);
+    for (int k = 0; k < 3; ++k) {
+        const unsigned long long x = warp_sum(acc[k]);
         if (lane == 0 && x)
-            atomicAdd(&bytes[t], x);
+            atomicAdd(&bytes[k], x);
     }
 }
 
@@ -656,28 +793,23 @@ struct TierSel {
 };
 
 // ---------------------------------------------------------------------------
-// launch helpers
+// launch helpers (one instantiation per depth)
 // ---------------------------------------------------------------------------
+#define BEEP_DEPTH_SWITCH(dend, CASE)                                                                              \
+    switch (dend) {                                                                                                \
+        CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10) default                                   \
+            : return fail(BEEP_ERR_UNSUPPORTED, "depth out of range");                                             \
+    }
+
 template <bool ENUM>
-beep_status launch_small(int dend, int grid, cudaStream_t s, const ViewDev &v, const DevPlan &pl, const uint32_t *roots,
-                         uint32_t n, int rev, unsigned long long *counter, const EnumDev &en) {
-    switch (dend) {
+beep_status launch_small(int dend, int grid, cudaStream_t s, const PairDev *pairs, const uint64_t *items,
+                         uint32_t n) {
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
-        k_small<D, ENUM><<<grid, kSmallWarps * 32, 0, s>>>(v, pl, roots, n, rev, counter, en);                      \
+        k_small<D, ENUM><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n);                                        \
         break;
-        BEEP_CASE(3)
-        BEEP_CASE(4)
-        BEEP_CASE(5)
-        BEEP_CASE(6)
-        BEEP_CASE(7)
-        BEEP_CASE(8)
-        BEEP_CASE(9)
-        BEEP_CASE(10)
+    BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
 #undef BEEP_CASE
-    default:
-        return fail(BEEP_ERR_UNSUPPORTED, "depth out of range");
-    }
     BEEP_CUDA_TRY(cudaGetLastError());
     return BEEP_OK;
 }
@@ -688,52 +820,28 @@ template <int D, bool ENUM> beep_status set_medium_attr(size_t smem) {
 }
 
 template <bool ENUM>
-beep_status launch_medium(int dend, int grid, int block, size_t smem, cudaStream_t s, const ViewDev &v,
-                          const DevPlan &pl, const uint32_t *roots, uint32_t n, int rev, unsigned *cursor,
-                          unsigned long long *counter, const EnumDev &en, uint32_t maxD) {
-    switch (dend) {
+beep_status launch_medium(int dend, int grid, int block, size_t smem, cudaStream_t s, const PairDev *pairs,
+                          const uint64_t *items, uint32_t n, unsigned *cursor, uint32_t maxD) {
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
         BEEP_TRY((set_medium_attr<D, ENUM>(smem)));                                                                \
-        k_medium<D, ENUM><<<grid, block, smem, s>>>(v, pl, roots, n, rev, cursor, counter, en, maxD);                \
+        k_medium<D, ENUM><<<grid, block, smem, s>>>(pairs, items, n, cursor, maxD);                                 \
         break;
-        BEEP_CASE(3)
-        BEEP_CASE(4)
-        BEEP_CASE(5)
-        BEEP_CASE(6)
-        BEEP_CASE(7)
-        BEEP_CASE(8)
-        BEEP_CASE(9)
-        BEEP_CASE(10)
+    BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
 #undef BEEP_CASE
-    default:
-        return fail(BEEP_ERR_UNSUPPORTED, "depth out of range");
-    }
     BEEP_CUDA_TRY(cudaGetLastError());
     return BEEP_OK;
 }
 
 template <bool ENUM>
-beep_status launch_large_dfs(int dend, int grid, cudaStream_t s, const ViewDev &v, const DevPlan &pl, const Batch &bt,
-                             const uint32_t *arena, unsigned *cursor, unsigned long long *counter,
-                             const EnumDev &en) {
-    switch (dend) {
+beep_status launch_large_dfs(int dend, int grid, cudaStream_t s, const PairDev *pairs, const Batch &bt,
+                             const uint32_t *arena, unsigned *cursor) {
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
-        k_large_dfs<D, ENUM><<<grid, 256, 0, s>>>(v, pl, bt, arena, cursor, counter, en);                           \
+        k_large_dfs<D, ENUM><<<grid, 256, 0, s>>>(pairs, bt, arena, cursor);                                        \
         break;
-        BEEP_CASE(3)
-        BEEP_CASE(4)
-        BEEP_CASE(5)
-        BEEP_CASE(6)
-        BEEP_CASE(7)
-        BEEP_CASE(8)
-        BEEP_CASE(9)
-        BEEP_CASE(10)
+    BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
 #undef BEEP_CASE
-    default:
-        return fail(BEEP_ERR_UNSUPPORTED, "depth out of range");
-    }
     BEEP_CUDA_TRY(cudaGetLastError());
     return BEEP_OK;
 }
@@ -780,239 +888,610 @@ struct Timer {
 
 } // namespace
 
-beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t options, const EnumRequest *enreq,
-                      beep_stats *stats) {
+// ---------------------------------------------------------------------------
+// Plan and execution of a multi-pair call.
+//
+// plan_pairs does everything that needs the host: views, root classification
+// (one read-back of the tier sizes), sorted item lists and the batching of
+// large roots into arena-sized groups. It leaves a list of launches whose
+// buffers it owns. execute_plan replays that list as a stream-ordered
+// sequence of memsets and kernels with no host synchronisation, so it can be
+// captured once into a CUDA graph (capture_plan) and relaunched.
+// ---------------------------------------------------------------------------
+struct LaunchRec {
+    enum Kind { kSmall, kMedium, kLargeRows, kLargeDfs, kMemset } kind;
+    int dend = 0, grid = 0, block = 0;
+    size_t smem = 0;
+    const uint64_t *items = nullptr;
+    uint32_t n = 0, maxD = 0;
+    unsigned *cursor = nullptr;
+    Batch bt{};
+    void *mptr = nullptr;
+    size_t mbytes = 0;
+    double *sink = nullptr; // stats field this launch's time adds to
+};
+
+struct LaunchPlan {
+    Ctx *ctx = nullptr;
+    std::vector<std::shared_ptr<View>> views; // kept alive while the plan exists
+    std::vector<void *> allocs;
+    std::vector<uint32_t> live; // spec index of each device pair
+    uint32_t np = 0;
+    PairDev *d_pairs = nullptr;
+    uint64_t *d_offs = nullptr;
+    uint8_t *d_tier = nullptr;
+    uint64_t N = 0;
+    unsigned long long *d_counts = nullptr; // np counts, np tuple counters, 4 byte counters
+    unsigned *d_cursors = nullptr;
+    uint32_t ncursors = 0;
+    unsigned long long *h_counts = nullptr; // pinned mirror (np + 4): the context's buffer, or owned when captured
+    bool own_h_counts = false;
+    std::vector<LaunchRec> recs;
+    bool enumerate = false;
+    beep_stats st{};
+    cudaGraphExec_t exec = nullptr;
+    ~LaunchPlan() {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        for (void *p : allocs)
+            cudaFreeAsync(p, ctx->stream);
+        if (h_counts && own_h_counts)
+            cudaFreeHost(h_counts);
+    }
+    template <typename T> beep_status alloc(T *&out, size_t count) {
+        void *p = nullptr;
+        const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+        cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, ctx->pool, ctx->stream);
+        if (e != cudaSuccess)
+            return fail(e == cudaErrorMemoryAllocation ? BEEP_ERR_OUT_OF_MEMORY : BEEP_ERR_CUDA,
+                        std::string("device pool allocation of ") + std::to_string(bytes) + " bytes: " +
+                            cudaGetErrorString(e));
+        allocs.push_back(p);
+        out = static_cast<T *>(p);
+        return BEEP_OK;
+    }
+};
+
+void LaunchPlanDeleter::operator()(LaunchPlan *p) const { delete p; }
+
+beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out) {
     cudaStream_t s = ctx->stream;
-    beep_stats st;
+    LaunchPlanPtr lp(new LaunchPlan);
+    lp->ctx = ctx;
+    beep_stats &st = lp->st;
     std::memset(&st, 0, sizeof(st));
-    const DevPlan &pl = plan.dev;
-    Timer tm;
-    tm.on = (options & BEEP_OPT_TIMING) != 0;
-    tm.s = s;
-    st.cutoff = g->cutoff;
-    st.ascending = pl.asc;
-
-    const bool enumerate = enreq && enreq->k > 0 && enreq->d_out;
-    EnumDev en{nullptr, nullptr, 0};
-
-    BEEP_TRY(ctx->counter.reserve(512));
-    // u64 [8] count, [9] tuples reserved, [10..12] adjacency bytes by tier; u32 cursors at u64 [16..]
-    unsigned long long *d_cnt = ctx->counter.as<unsigned long long>() + 8;
-    unsigned *d_cursor = reinterpret_cast<unsigned *>(ctx->counter.as<unsigned long long>() + 16);
-    BEEP_CUDA_TRY(cudaMemsetAsync(d_cnt, 0, 8 * 8, s));
-    if (enumerate) {
-        en.out = enreq->d_out;
-        en.n = d_cnt + 1;
-        en.k = enreq->k;
+    if (!specs.empty()) {
+        st.cutoff = specs[0].g->cutoff;
+        st.ascending = specs[0].plan.dev.asc;
     }
-
-    if (g->n == 0 || pl.dend < 3) {
-        // sgc with K - LUNMAT < 3: the reference's main path never reaches a
-        // counting level (check_terminate/backtrack need l >= 3).
-        if (stats)
-            *stats = st;
+    // views (peel + priority relabelling, cached per graph)
+    std::vector<PairDev> hp;
+    std::vector<uint64_t> offs{0};
+    std::vector<Graph *> dropped;
+    for (size_t i = 0; i < specs.size(); ++i) {
+        const PairSpec &ps = specs[i];
+        if (ps.g->n == 0 || ps.plan.dev.dend < 3)
+            continue; // K - LUNMAT < 3: the reference's main path never reaches a counting level
+        if ((options & BEEP_OPT_NO_VIEW_CACHE) && std::find(dropped.begin(), dropped.end(), ps.g) == dropped.end()) {
+            ps.g->views.clear();
+            dropped.push_back(ps.g);
+        }
+        std::shared_ptr<View> v;
+        bool built = false;
+        BEEP_TRY(get_view(ctx, ps.g, ps.plan.info.min_qdeg, ps.plan.dev.asc, false, &v, &built));
+        lp->views.push_back(v);
+        st.peel_rounds = v->peel_rounds; // view-build launches are counted where they happen
+        if (v->n == 0)
+            continue;
+        PairDev pd;
+        std::memset(&pd, 0, sizeof(pd));
+        pd.v = ViewDev{v->row_ptr.as<uint32_t>(), v->col.as<uint32_t>(), v->split.as<uint32_t>(),
+                       v->orig.as<uint32_t>()};
+        pd.pl = ps.plan.dev;
+        pd.min_deg = (uint32_t)ps.plan.info.max_qdeg;
+        pd.cap_deg = (options & BEEP_OPT_REFERENCE_ROOT_CAP)
+                         ? (uint32_t)std::min<uint64_t>(0xffffffffull, (uint64_t)ps.g->cutoff * 100ull)
+                         : 0xffffffffu;
+        if (ps.en && ps.en->k > 0 && ps.en->d_out) {
+            lp->enumerate = true;
+            pd.en.out = ps.en->d_out;
+            pd.en.k = ps.en->k;
+        }
+        hp.push_back(pd);
+        lp->live.push_back((uint32_t)i);
+        offs.push_back(offs.back() + (uint64_t)v->n);
+    }
+    const uint32_t np = (uint32_t)hp.size();
+    lp->np = np;
+    BEEP_TRY(ctx->host_results(np + 4, &lp->h_counts));
+    BEEP_TRY(lp->alloc(lp->d_counts, 2 * (size_t)np + 4));
+    lp->ncursors = 64;
+    BEEP_TRY(lp->alloc(lp->d_cursors, lp->ncursors));
+    if (np == 0) {
+        *out = std::move(lp);
         return BEEP_OK;
     }
-
-    // peel + priority relabelling (cached per (min_qdeg, order))
-    int tprep = tm.start();
-    View *v = nullptr;
-    bool built = false;
-    BEEP_TRY(get_view(ctx, g, plan.info.min_qdeg, pl.asc, (options & BEEP_OPT_NO_VIEW_CACHE) != 0, &v, &built,
-                      nullptr));
-    tm.stop(tprep, &st.prep_ms);
-    st.peel_rounds = v->peel_rounds;
-    if (built)
-        st.kernel_launches += 8 + 2 * v->peel_rounds;
-    if (v->n == 0) {
-        tm.collect();
-        if (stats)
-            *stats = st;
-        return BEEP_OK;
+    const uint64_t N = offs.back();
+    if (N >= 0xffffffffull)
+        return fail(BEEP_ERR_UNSUPPORTED, "more than 2^32 vertices in one call");
+    lp->N = N;
+    for (uint32_t i = 0; i < np; ++i) {
+        hp[i].count = lp->d_counts + i;
+        if (hp[i].en.out)
+            hp[i].en.n = lp->d_counts + np + i;
     }
-    ViewDev vd{v->row_ptr.as<uint32_t>(), v->col.as<uint32_t>(), v->split.as<uint32_t>(), v->orig.as<uint32_t>()};
-    const int64_t n = v->n;
-
-    // classify roots into tiers
-    size_t need = (size_t)n * 1 + 256 + (size_t)n * 4 * 8 + 4096;
-    BEEP_TRY(ctx->scratch2.reserve(need));
-    char *base = ctx->scratch2.as<char>();
-    uint8_t *tier = reinterpret_cast<uint8_t *>(base);
-    uint32_t *dom = reinterpret_cast<uint32_t *>(base + (((size_t)n + 255) & ~(size_t)255));
-    uint32_t *lists[4]; // small, medium (<= 256), medium (<= 1024), large
-    for (int t = 0; t < 4; ++t)
-        lists[t] = dom + (size_t)n * (t + 1);
-    uint32_t *d_nsel = dom + (size_t)n * 5;       // [0..3] counts, [4..7] max domain per tier
-    uint32_t *d_gD = dom + (size_t)n * 5 + 64;     // large-tier gather
-    uint32_t *d_gj = d_gD + (size_t)n;
-    BEEP_CUDA_TRY(cudaMemsetAsync(d_nsel, 0, 64, s));
-    uint64_t cap_deg = 0xffffffffull;
-    if (options & BEEP_OPT_REFERENCE_ROOT_CAP)
-        cap_deg = std::min<uint64_t>(0xffffffffull, (uint64_t)g->cutoff * 100ull);
-    int tcount = tm.start();
-    const int gv = std::max(1, (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 32));
-    k_classify<<<gv, 256, 0, s>>>(vd, pl, n, (uint32_t)plan.info.max_qdeg, (uint32_t)cap_deg, tier, dom,
-                                  d_nsel + 4);
+    BEEP_TRY(lp->alloc(lp->d_pairs, np));
+    BEEP_TRY(lp->alloc(lp->d_offs, np + 1));
+    BEEP_TRY(lp->alloc(lp->d_tier, N));
+    uint32_t *d_dom, *d_sel, *d_keys, *d_keys2;
+    unsigned *d_misc;
+    uint64_t *d_tmp_items;
+    BEEP_TRY(lp->alloc(d_dom, N));
+    BEEP_TRY(lp->alloc(d_sel, N));
+    BEEP_TRY(lp->alloc(d_keys, N));
+    BEEP_TRY(lp->alloc(d_keys2, N));
+    BEEP_TRY(lp->alloc(d_misc, 256));
+    BEEP_TRY(lp->alloc(d_tmp_items, N));
+    BEEP_CUDA_TRY(cudaMemcpyAsync(lp->d_pairs, hp.data(), np * sizeof(PairDev), cudaMemcpyHostToDevice, s));
+    BEEP_CUDA_TRY(cudaMemcpyAsync(lp->d_offs, offs.data(), (np + 1) * 8, cudaMemcpyHostToDevice, s));
+    BEEP_CUDA_TRY(cudaMemsetAsync(d_misc, 0, 256 * 4, s));
+    const int gv = std::max(1, (int)std::min<uint64_t>((N + 255) / 256, (uint64_t)ctx->num_sms * 32));
+    k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, lp->d_tier, d_dom, d_misc, d_misc + 4);
     BEEP_CUDA_TRY(cudaGetLastError());
     st.kernel_launches += 1;
-    uint32_t nsel[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int t = 0; t < 4; ++t) {
+    unsigned h_misc[64];
+    BEEP_CUDA_TRY(cudaMemcpyAsync(h_misc, d_misc, sizeof(h_misc), cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    const unsigned *tier_max = h_misc;
+    const unsigned *tier_depth = h_misc + 4;
+    uint32_t tier_n[kTiers];
+    for (int k = 0; k < kTiers; ++k) {
+        tier_n[k] = 0;
+        for (int d = 0; d < kDepths; ++d)
+            tier_n[k] += tier_depth[k * kDepths + d];
+    }
+    st.roots_small = tier_n[0];
+    st.roots_medium = (int64_t)tier_n[1] + tier_n[2];
+    st.roots_large = tier_n[3];
+    st.roots = st.roots_small + st.roots_medium + st.roots_large;
+    uint32_t next_cursor = 0;
+    auto cursor = [&]() -> unsigned * { return lp->d_cursors + (next_cursor++ % lp->ncursors); };
+
+    // item list of tier k in its own buffer, sorted by depth (medium: largest domain first)
+    auto make_list = [&](int k, uint64_t *&list) -> beep_status {
+        const uint32_t n_k = tier_n[k];
+        BEEP_TRY(lp->alloc(list, n_k));
         size_t tb = 0;
         cub::CountingInputIterator<uint32_t> it(0);
-        TierSel sel{tier, (uint8_t)(t + 1)};
-        BEEP_CUDA_TRY(cub::DeviceSelect::If(nullptr, tb, it, lists[t], d_nsel + t, n, sel, s));
+        TierSel sel{lp->d_tier, (uint8_t)(k + 1)};
+        unsigned *d_ns = d_misc + 80;
+        BEEP_CUDA_TRY(cub::DeviceSelect::If(nullptr, tb, it, d_sel, d_ns, N, sel, s));
         BEEP_TRY(ctx->scratch.reserve(tb + 1024));
-        BEEP_CUDA_TRY(cub::DeviceSelect::If(ctx->scratch.ptr, tb, it, lists[t], d_nsel + t, n, sel, s));
+        BEEP_CUDA_TRY(cub::DeviceSelect::If(ctx->scratch.ptr, tb, it, d_sel, d_ns, N, sel, s));
+        const int by_domain = (k == 1 || k == 2) ? 1 : 0;
+        int depths = 0;
+        for (int d = 0; d < kDepths; ++d)
+            depths += tier_depth[k * kDepths + d] > 0;
+        const bool sort = depths > 1 || by_domain;
+        k_make_items<<<std::max(1u, std::min(n_k / 256 + 1, 4096u)), 256, 0, s>>>(
+            d_sel, n_k, lp->d_pairs, lp->d_offs, np, d_dom, by_domain, sort ? d_tmp_items : list, d_keys);
+        BEEP_CUDA_TRY(cudaGetLastError());
         st.kernel_launches += 1;
-    }
-    BEEP_CUDA_TRY(cudaMemcpyAsync(nsel, d_nsel, sizeof(nsel), cudaMemcpyDeviceToHost, s));
-    const uint32_t max_medA = nsel[5], max_medB = nsel[6];
-    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
-    st.roots_small = nsel[0];
-    st.roots_medium = (int64_t)nsel[1] + nsel[2];
-    st.roots_large = nsel[3];
-    st.roots = (int64_t)nsel[0] + nsel[1] + nsel[2] + nsel[3];
-    // heaviest roots first: in ascending order they have the largest ids
-    const int rev = pl.asc ? 1 : 0;
-    BEEP_CUDA_TRY(cudaMemsetAsync(d_cursor, 0, 16, s));
+        if (sort) {
+            tb = 0;
+            const int end_bit = by_domain ? 20 : 4;
+            BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_keys, d_keys2, d_tmp_items, list, n_k, 0,
+                                                          end_bit, s));
+            BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+            BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ctx->scratch.ptr, tb, d_keys, d_keys2, d_tmp_items, list,
+                                                          n_k, 0, end_bit, s));
+        }
+        return BEEP_OK;
+    };
 
     // large tier: batches of roots whose bitmaps fit the arena
-    if (nsel[3] > 0) {
-        std::vector<uint32_t> lr(nsel[3]), lD(nsel[3]), lj(nsel[3]);
-        k_gather_dom<<<std::max(1u, std::min(nsel[3] / 256 + 1, 1024u)), 256, 0, s>>>(vd, pl, lists[3], nsel[3], d_gD,
-                                                                                      d_gj);
+    if (tier_n[3] > 0) {
+        uint64_t *list = nullptr;
+        BEEP_TRY(make_list(3, list));
+        const uint32_t nl = tier_n[3];
+        std::vector<uint64_t> litems(nl);
+        std::vector<uint32_t> lD(nl), lj(nl);
+        k_gather_dom<<<std::max(1u, std::min(nl / 256 + 1, 1024u)), 256, 0, s>>>(lp->d_pairs, list, nl, d_keys,
+                                                                               d_sel);
         BEEP_CUDA_TRY(cudaGetLastError());
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lr.data(), lists[3], 4ull * nsel[3], cudaMemcpyDeviceToHost, s));
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lD.data(), d_gD, 4ull * nsel[3], cudaMemcpyDeviceToHost, s));
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lj.data(), d_gj, 4ull * nsel[3], cudaMemcpyDeviceToHost, s));
-        BEEP_CUDA_TRY(cudaStreamSynchronize(s));
         st.kernel_launches += 1;
+        BEEP_CUDA_TRY(cudaMemcpyAsync(litems.data(), list, 8ull * nl, cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lD.data(), d_keys, 4ull * nl, cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lj.data(), d_sel, 4ull * nl, cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaStreamSynchronize(s));
         struct R {
-            uint32_t r, D, j0;
+            uint64_t item;
+            uint32_t D, j0, dend;
         };
-        std::vector<R> rs(nsel[3]);
-        for (uint32_t i = 0; i < nsel[3]; ++i)
-            rs[i] = R{lr[i], lD[i], lj[i]};
+        std::vector<R> rs(nl);
+        for (uint32_t i = 0; i < nl; ++i)
+            rs[i] = R{litems[i], lD[i], lj[i], (uint32_t)hp[(uint32_t)(litems[i] >> 32)].pl.dend};
         std::sort(rs.begin(), rs.end(), [](const R &a, const R &b) { return a.D > b.D; });
         size_t free_b = 0, total_b = 0;
         BEEP_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-        size_t arena_cap = std::max<size_t>((size_t)256 << 20, std::min<size_t>((size_t)48 << 30, free_b / 2 +
-                                                                                       ctx->arena.bytes));
-        size_t i0 = 0;
-        while (i0 < rs.size()) {
+        const size_t arena_cap = std::max<size_t>((size_t)256 << 20, std::min<size_t>((size_t)48 << 30, free_b / 2));
+        // batch boundaries and the arena size (largest batch)
+        std::vector<std::pair<size_t, size_t>> batches;
+        size_t arena_words = 0;
+        for (size_t i0 = 0; i0 < rs.size();) {
             size_t words = 0, i1 = i0;
-            std::vector<uint32_t> broot, cstart{0}, tstart{0};
-            std::vector<uint64_t> boff;
             while (i1 < rs.size()) {
-                const uint64_t W = (rs[i1].D + 31) / 32;
-                const uint64_t w = (uint64_t)rs[i1].D * W;
+                const uint64_t w = ((uint64_t)rs[i1].D * ((rs[i1].D + 31) / 32) + 31) & ~(uint64_t)31;
                 if (i1 > i0 && (words + w) * 4 > arena_cap)
                     break;
-                broot.push_back(rs[i1].r);
-                boff.push_back(words);
-                words += (w + 31) & ~(uint64_t)31; // 128-byte aligned rows
-                cstart.push_back(cstart.back() + (rs[i1].D + kRowsPerChunk - 1) / kRowsPerChunk);
-                tstart.push_back(tstart.back() + (rs[i1].D - rs[i1].j0));
+                words += w;
                 ++i1;
             }
             if (words * 4 > arena_cap)
                 return fail(BEEP_ERR_OUT_OF_MEMORY, "a root's neighbourhood bitmap (" + std::to_string(words * 4) +
                                                         " bytes) exceeds the bitmap arena");
-            BEEP_TRY(ctx->arena.reserve(words * 4));
-            // batch descriptors
-            const uint32_t nb = (uint32_t)broot.size();
-            size_t dbytes = nb * 4 + nb * 8 + (nb + 1) * 8 + 1024;
-            BEEP_TRY(ctx->scratch.reserve(dbytes));
-            char *db = ctx->scratch.as<char>();
-            uint64_t *d_off = reinterpret_cast<uint64_t *>(db);
-            uint32_t *d_root = reinterpret_cast<uint32_t *>(db + nb * 8);
-            uint32_t *d_cs = d_root + nb;
-            uint32_t *d_ts = d_cs + nb + 1;
-            BEEP_CUDA_TRY(cudaMemcpyAsync(d_off, boff.data(), nb * 8, cudaMemcpyHostToDevice, s));
-            BEEP_CUDA_TRY(cudaMemcpyAsync(d_root, broot.data(), nb * 4, cudaMemcpyHostToDevice, s));
-            BEEP_CUDA_TRY(cudaMemcpyAsync(d_cs, cstart.data(), (nb + 1) * 4, cudaMemcpyHostToDevice, s));
-            BEEP_CUDA_TRY(cudaMemcpyAsync(d_ts, tstart.data(), (nb + 1) * 4, cudaMemcpyHostToDevice, s));
-            BEEP_CUDA_TRY(cudaMemsetAsync(ctx->arena.ptr, 0, words * 4, s));
-            BEEP_CUDA_TRY(cudaMemsetAsync(d_cursor, 0, 16, s));
-            st.bitmap_bytes += words * 4;
-            Batch bt{d_root, d_off, d_cs, d_ts, nb};
-            uint32_t maxD = rs[i0].D;
-            size_t smemA = std::min<size_t>(maxD, kLargeSmemA) * 4;
-            BEEP_CUDA_TRY(cudaFuncSetAttribute(k_large_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemA));
-            int te = tm.start();
-            k_large_rows<<<ctx->num_sms, 512, smemA, s>>>(vd, pl, bt, ctx->arena.as<uint32_t>(), d_cursor);
-            BEEP_CUDA_TRY(cudaGetLastError());
-            tm.stop(te, &st.large_encode_ms);
-            int td = tm.start();
-            if (enumerate)
-                BEEP_TRY(launch_large_dfs<true>(pl.dend, ctx->num_sms * 8, s, vd, pl, bt, ctx->arena.as<uint32_t>(),
-                                                d_cursor + 1, d_cnt, en));
-            else
-                BEEP_TRY(launch_large_dfs<false>(pl.dend, ctx->num_sms * 8, s, vd, pl, bt, ctx->arena.as<uint32_t>(),
-                                                 d_cursor + 1, d_cnt, en));
-            tm.stop(td, &st.large_dfs_ms);
-            st.large_encode_launches++;
-            st.large_dfs_launches++;
-            st.kernel_launches += 2;
-            BEEP_CUDA_TRY(cudaStreamSynchronize(s)); // arena reuse by the next batch
+            arena_words = std::max(arena_words, words);
+            batches.push_back({i0, i1});
             i0 = i1;
         }
-        BEEP_CUDA_TRY(cudaMemsetAsync(d_cursor, 0, 16, s));
+        uint32_t *arena = nullptr;
+        BEEP_TRY(lp->alloc(arena, arena_words));
+        const uint32_t maxD_all = rs[0].D;
+        const size_t smemA = std::min<size_t>(maxD_all, kLargeSmemA) * 4;
+        BEEP_CUDA_TRY(cudaFuncSetAttribute(k_large_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemA));
+        for (auto &bb : batches) {
+            const size_t i0 = bb.first, i1 = bb.second;
+            std::stable_sort(rs.begin() + i0, rs.begin() + i1,
+                             [](const R &a, const R &b) { return a.dend < b.dend; });
+            const uint32_t nbt = (uint32_t)(i1 - i0);
+            std::vector<uint64_t> bitem, boff;
+            std::vector<uint32_t> cstart{0};
+            uint64_t words = 0;
+            for (size_t i = i0; i < i1; ++i) {
+                bitem.push_back(rs[i].item);
+                boff.push_back(words);
+                words += ((uint64_t)rs[i].D * ((rs[i].D + 31) / 32) + 31) & ~(uint64_t)31;
+                cstart.push_back(cstart.back() + (rs[i].D + kRowsPerChunk - 1) / kRowsPerChunk);
+            }
+            std::vector<std::pair<uint32_t, uint32_t>> groups; // (first entry, count) per depth
+            for (uint32_t a = 0; a < nbt;) {
+                uint32_t b = a;
+                while (b < nbt && rs[i0 + b].dend == rs[i0 + a].dend)
+                    ++b;
+                groups.push_back({a, b - a});
+                a = b;
+            }
+            std::vector<uint32_t> ts_all, ts_off;
+            for (auto &gp : groups) {
+                ts_off.push_back((uint32_t)ts_all.size());
+                uint32_t acc = 0;
+                ts_all.push_back(0);
+                for (uint32_t e = 0; e < gp.second; ++e) {
+                    const R &x = rs[i0 + gp.first + e];
+                    acc += x.D - x.j0;
+                    ts_all.push_back(acc);
+                }
+            }
+            uint64_t *d_bitem, *d_boff;
+            uint32_t *d_cs, *d_ts;
+            BEEP_TRY(lp->alloc(d_bitem, nbt));
+            BEEP_TRY(lp->alloc(d_boff, nbt));
+            BEEP_TRY(lp->alloc(d_cs, nbt + 1));
+            BEEP_TRY(lp->alloc(d_ts, ts_all.size()));
+            BEEP_CUDA_TRY(cudaMemcpyAsync(d_bitem, bitem.data(), nbt * 8, cudaMemcpyHostToDevice, s));
+            BEEP_CUDA_TRY(cudaMemcpyAsync(d_boff, boff.data(), nbt * 8, cudaMemcpyHostToDevice, s));
+            BEEP_CUDA_TRY(cudaMemcpyAsync(d_cs, cstart.data(), (nbt + 1) * 4, cudaMemcpyHostToDevice, s));
+            BEEP_CUDA_TRY(cudaMemcpyAsync(d_ts, ts_all.data(), ts_all.size() * 4, cudaMemcpyHostToDevice, s));
+            LaunchRec ms;
+            ms.kind = LaunchRec::kMemset;
+            ms.mptr = arena;
+            ms.mbytes = words * 4;
+            lp->recs.push_back(ms);
+            st.bitmap_bytes += words * 4;
+            LaunchRec lr;
+            lr.kind = LaunchRec::kLargeRows;
+            lr.grid = ctx->num_sms;
+            lr.block = 512;
+            lr.smem = smemA;
+            lr.bt = Batch{d_bitem, d_boff, d_cs, d_ts, nbt};
+            lr.mptr = arena;
+            lr.cursor = cursor();
+            lr.sink = &st.large_encode_ms;
+            lp->recs.push_back(lr);
+            for (size_t gi = 0; gi < groups.size(); ++gi) {
+                LaunchRec ld;
+                ld.kind = LaunchRec::kLargeDfs;
+                ld.dend = (int)rs[i0 + groups[gi].first].dend;
+                ld.grid = ctx->num_sms * 8;
+                ld.block = 256;
+                ld.bt = Batch{d_bitem + groups[gi].first, d_boff + groups[gi].first, d_cs, d_ts + ts_off[gi],
+                              groups[gi].second};
+                ld.mptr = arena;
+                ld.cursor = cursor();
+                ld.sink = &st.large_dfs_ms;
+                lp->recs.push_back(ld);
+            }
+        }
     }
     // medium tiers: block per root, bitmap in shared memory
     for (int sub = 0; sub < 2; ++sub) {
-        const uint32_t nm = nsel[1 + sub];
-        if (nm == 0)
+        const int k = 1 + sub;
+        if (tier_n[k] == 0)
             continue;
-        const uint32_t maxD = sub == 0 ? max_medA : max_medB;
+        uint64_t *list = nullptr;
+        BEEP_TRY(make_list(k, list));
+        const uint32_t maxD = tier_max[k];
         const uint32_t W = (maxD + 31) / 32;
         const size_t pad = (maxD + 4) & ~3u;
         const size_t smem = (3 * pad + (size_t)maxD * W) * 4;
         const int block = sub == 0 ? 256 : 1024;
         const int per_sm = std::max(1, (int)std::min<size_t>(2048 / block, (200 * 1024) / (smem + 1024)));
-        const int grid = ctx->num_sms * per_sm;
-        int tmid = tm.start();
-        if (enumerate)
-            BEEP_TRY(launch_medium<true>(pl.dend, grid, block, smem, s, vd, pl, lists[1 + sub], nm, rev,
-                                         d_cursor + 2 + sub, d_cnt, en, maxD));
-        else
-            BEEP_TRY(launch_medium<false>(pl.dend, grid, block, smem, s, vd, pl, lists[1 + sub], nm, rev,
-                                          d_cursor + 2 + sub, d_cnt, en, maxD));
-        tm.stop(tmid, &st.medium_ms);
-        st.medium_launches++;
-        st.kernel_launches += 1;
+        uint32_t first = 0;
+        for (int d = 3; d < kDepths; ++d) {
+            const uint32_t cnt = tier_depth[k * kDepths + d];
+            if (!cnt)
+                continue;
+            LaunchRec r;
+            r.kind = LaunchRec::kMedium;
+            r.dend = d;
+            r.grid = ctx->num_sms * per_sm;
+            r.block = block;
+            r.smem = smem;
+            r.items = list + first;
+            r.n = cnt;
+            r.maxD = maxD;
+            r.cursor = cursor();
+            r.sink = &st.medium_ms;
+            lp->recs.push_back(r);
+            first += cnt;
+        }
     }
     // small tier
-    if (nsel[0] > 0) {
-        int grid = (int)std::min<int64_t>(((int64_t)nsel[0] + kSmallWarps - 1) / kSmallWarps,
-                                          (int64_t)ctx->num_sms * 8);
-        int tsm = tm.start();
-        if (enumerate)
-            BEEP_TRY(launch_small<true>(pl.dend, grid, s, vd, pl, lists[0], nsel[0], rev, d_cnt, en));
-        else
-            BEEP_TRY(launch_small<false>(pl.dend, grid, s, vd, pl, lists[0], nsel[0], rev, d_cnt, en));
-        tm.stop(tsm, &st.small_ms);
-        st.small_launches++;
-        st.kernel_launches += 1;
+    if (tier_n[0] > 0) {
+        uint64_t *list = nullptr;
+        BEEP_TRY(make_list(0, list));
+        uint32_t first = 0;
+        for (int d = 3; d < kDepths; ++d) {
+            const uint32_t cnt = tier_depth[d];
+            if (!cnt)
+                continue;
+            LaunchRec r;
+            r.kind = LaunchRec::kSmall;
+            r.dend = d;
+            r.grid = (int)std::min<int64_t>(((int64_t)cnt + kSmallWarps - 1) / kSmallWarps, (int64_t)ctx->num_sms * 8);
+            r.block = kSmallWarps * 32;
+            r.items = list + first;
+            r.n = cnt;
+            r.sink = &st.small_ms;
+            lp->recs.push_back(r);
+            first += cnt;
+        }
     }
-    tm.stop(tcount, &st.count_ms);
-    if (options & BEEP_OPT_ALG_BYTES) {
-        k_alg_bytes<<<gv, 256, 0, s>>>(vd, pl, tier, n, d_cnt + 2);
+    // shared-memory opt-ins are host calls: done here, never inside a capture
+    for (auto &r : lp->recs)
+        if (r.kind == LaunchRec::kMedium) {
+#define BEEP_CASE(D)                                                                                               \
+    case D:                                                                                                        \
+        if (lp->enumerate)                                                                                         \
+            BEEP_TRY((set_medium_attr<D, true>(r.smem)));                                                          \
+        else                                                                                                       \
+            BEEP_TRY((set_medium_attr<D, false>(r.smem)));                                                         \
+        break;
+            BEEP_DEPTH_SWITCH(r.dend, BEEP_CASE)
+#undef BEEP_CASE
+        }
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s)); // planning buffers are final
+    *out = std::move(lp);
+    return BEEP_OK;
+}
+
+namespace {
+beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::vector<std::pair<cudaEvent_t, cudaEvent_t>> *ev,
+                  std::vector<double *> *sinks) {
+    cudaStream_t s = ctx->stream;
+    const uint32_t np = lp->np;
+    BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_counts, 0, (2 * (size_t)np + 4) * 8, s));
+    BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_cursors, 0, lp->ncursors * 4, s));
+    for (auto &r : lp->recs) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (timing && r.sink) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, s);
+        }
+        switch (r.kind) {
+        case LaunchRec::kMemset:
+            BEEP_CUDA_TRY(cudaMemsetAsync(r.mptr, 0, r.mbytes, s));
+            break;
+        case LaunchRec::kLargeRows:
+            k_large_rows<<<r.grid, r.block, r.smem, s>>>(lp->d_pairs, r.bt, static_cast<uint32_t *>(r.mptr), r.cursor);
+            BEEP_CUDA_TRY(cudaGetLastError());
+            st.large_encode_launches++;
+            break;
+        case LaunchRec::kLargeDfs:
+            if (lp->enumerate)
+                BEEP_TRY(launch_large_dfs<true>(r.dend, r.grid, s, lp->d_pairs, r.bt,
+                                                static_cast<const uint32_t *>(r.mptr), r.cursor));
+            else
+                BEEP_TRY(launch_large_dfs<false>(r.dend, r.grid, s, lp->d_pairs, r.bt,
+                                                 static_cast<const uint32_t *>(r.mptr), r.cursor));
+            st.large_dfs_launches++;
+            break;
+        case LaunchRec::kMedium:
+#define BEEP_CASE(D)                                                                                               \
+    case D:                                                                                                        \
+        if (lp->enumerate)                                                                                         \
+            k_medium<D, true><<<r.grid, r.block, r.smem, s>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);        \
+        else                                                                                                       \
+            k_medium<D, false><<<r.grid, r.block, r.smem, s>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);       \
+        break;
+            BEEP_DEPTH_SWITCH(r.dend, BEEP_CASE)
+#undef BEEP_CASE
+            BEEP_CUDA_TRY(cudaGetLastError());
+            st.medium_launches++;
+            break;
+        case LaunchRec::kSmall:
+            if (lp->enumerate)
+                BEEP_TRY(launch_small<true>(r.dend, r.grid, s, lp->d_pairs, r.items, r.n));
+            else
+                BEEP_TRY(launch_small<false>(r.dend, r.grid, s, lp->d_pairs, r.items, r.n));
+            st.small_launches++;
+            break;
+        }
+        if (r.kind != LaunchRec::kMemset)
+            st.kernel_launches += 1;
+        if (a) {
+            cudaEventRecord(b, s);
+            ev->push_back({a, b});
+            sinks->push_back(r.sink);
+        }
+    }
+    return BEEP_OK;
+}
+} // namespace
+
+beep_status capture_plan(Ctx *ctx, LaunchPlan *lp) {
+    if (lp->exec)
+        return BEEP_OK;
+    cudaStream_t s = ctx->stream;
+    // the captured read-back needs a host buffer that no other call reuses
+    if (!lp->own_h_counts) {
+        unsigned long long *h = nullptr;
+        BEEP_CUDA_TRY(cudaMallocHost(&h, (lp->np + 4) * sizeof(unsigned long long)));
+        lp->h_counts = h;
+        lp->own_h_counts = true;
+    }
+    beep_stats scratch_st;
+    std::memset(&scratch_st, 0, sizeof(scratch_st));
+    cudaGraph_t graph = nullptr;
+    BEEP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    beep_status rc = issue(ctx, lp, false, scratch_st, nullptr, nullptr);
+    cudaError_t ce = cudaMemcpyAsync(lp->h_counts, lp->d_counts, (lp->np + 4) * 8, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamEndCapture(s, &graph);
+    if (rc != BEEP_OK) {
+        if (graph)
+            cudaGraphDestroy(graph);
+        return rc;
+    }
+    BEEP_CUDA_TRY(ce);
+    BEEP_CUDA_TRY(e);
+    e = cudaGraphInstantiate(&lp->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    BEEP_CUDA_TRY(e);
+    return BEEP_OK;
+}
+
+beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::vector<PairSpec> *specs_unused,
+                         uint64_t *counts, size_t ncounts, beep_stats *stats) {
+    (void)specs_unused;
+    cudaStream_t s = ctx->stream;
+    beep_stats st = lp->st;
+    const bool timing = (options & BEEP_OPT_TIMING) != 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    std::vector<double *> sinks;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timing) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, s);
+    }
+    if (lp->exec) {
+        BEEP_CUDA_TRY(cudaGraphLaunch(lp->exec, s));
+        st.kernel_launches = 0;
+        for (auto &r : lp->recs)
+            st.kernel_launches += r.kind != LaunchRec::kMemset;
+    } else {
+        st.kernel_launches = lp->st.kernel_launches;
+        BEEP_TRY(issue(ctx, lp, timing, st, &ev, &sinks));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, (lp->np + 4) * 8, cudaMemcpyDeviceToHost, s));
+    }
+    if (timing)
+        cudaEventRecord(e1, s);
+    if (lp->np > 0 && (options & BEEP_OPT_ALG_BYTES)) {
+        unsigned long long *d_bytes = lp->d_counts + 2 * (size_t)lp->np;
+        BEEP_CUDA_TRY(cudaMemsetAsync(d_bytes, 0, 32, s));
+        const int gv = std::max(1, (int)std::min<uint64_t>((lp->N + 255) / 256, (uint64_t)ctx->num_sms * 32));
+        k_alg_bytes<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, lp->np, lp->d_tier, lp->N, d_bytes);
         BEEP_CUDA_TRY(cudaGetLastError());
         st.kernel_launches += 1;
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts + lp->np, d_bytes, 32, cudaMemcpyDeviceToHost, s));
     }
-    unsigned long long h[5] = {0, 0, 0, 0, 0};
-    BEEP_CUDA_TRY(cudaMemcpyAsync(h, d_cnt, sizeof(h), cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
-    tm.collect();
-    st.count = h[0];
-    st.small_bytes = h[2];
-    st.medium_bytes = h[3];
-    st.large_bytes = h[4];
-    st.adjacency_bytes = h[2] + h[3] + h[4];
+    if (timing) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        st.count_ms = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        for (size_t i = 0; i < ev.size(); ++i) {
+            cudaEventElapsedTime(&ms, ev[i].first, ev[i].second);
+            *sinks[i] += ms;
+            cudaEventDestroy(ev[i].first);
+            cudaEventDestroy(ev[i].second);
+        }
+        // sinks point into lp->st; report through st
+        st.small_ms = lp->st.small_ms;
+        st.medium_ms = lp->st.medium_ms;
+        st.large_encode_ms = lp->st.large_encode_ms;
+        st.large_dfs_ms = lp->st.large_dfs_ms;
+        lp->st.small_ms = lp->st.medium_ms = lp->st.large_encode_ms = lp->st.large_dfs_ms = 0;
+    }
+    for (size_t i = 0; i < ncounts; ++i)
+        counts[i] = 0;
+    st.count = 0;
+    for (uint32_t i = 0; i < lp->np; ++i) {
+        if (lp->live[i] < ncounts)
+            counts[lp->live[i]] = lp->h_counts[i];
+        st.count += lp->h_counts[i];
+    }
+    if (options & BEEP_OPT_ALG_BYTES) {
+        st.small_bytes = lp->h_counts[lp->np + 0];
+        st.medium_bytes = lp->h_counts[lp->np + 1];
+        st.large_bytes = lp->h_counts[lp->np + 2];
+        st.adjacency_bytes = st.small_bytes + st.medium_bytes + st.large_bytes;
+    }
     if (stats)
         *stats = st;
     return BEEP_OK;
+}
+
+beep_status run_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, beep_stats *stats,
+                      uint64_t *counts) {
+    cudaEvent_t p0 = nullptr, p1 = nullptr;
+    const bool timing = (options & BEEP_OPT_TIMING) != 0;
+    if (timing) {
+        cudaEventCreate(&p0);
+        cudaEventCreate(&p1);
+        cudaEventRecord(p0, ctx->stream);
+    }
+    LaunchPlanPtr lp;
+    BEEP_TRY(plan_pairs(ctx, specs, options, &lp));
+    double prep_ms = 0;
+    if (timing) {
+        cudaEventRecord(p1, ctx->stream);
+        cudaEventSynchronize(p1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p0, p1);
+        prep_ms = ms;
+        cudaEventDestroy(p0);
+        cudaEventDestroy(p1);
+    }
+    beep_stats st;
+    BEEP_TRY(execute_plan(ctx, lp.get(), options, &specs, counts, specs.size(), &st));
+    st.prep_ms = prep_ms;
+    if (stats)
+        *stats = st;
+    return BEEP_OK;
+}
+
+beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t options, const EnumRequest *enreq,
+                      beep_stats *stats) {
+    std::vector<PairSpec> one(1);
+    one[0].g = g;
+    one[0].plan = plan;
+    one[0].en = enreq;
+    uint64_t c = 0;
+    return run_pairs(ctx, one, options, stats, &c);
 }
 
 } // namespace beep

@@ -537,22 +537,22 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
 
 } // namespace
 
-beep_status get_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, bool no_cache, View **out, bool *built,
-                     cudaEvent_t) {
+beep_status get_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, bool no_cache,
+                     std::shared_ptr<View> *out, bool *built) {
     auto key = std::make_pair((int)min_qdeg, (int)asc);
     if (no_cache)
         g->views.erase(key);
     auto it = g->views.find(key);
     if (it != g->views.end()) {
-        *out = it->second.get();
+        *out = it->second;
         if (built)
             *built = false;
         return BEEP_OK;
     }
-    auto v = std::make_unique<View>();
+    auto v = std::make_shared<View>();
     BEEP_TRY(build_view(ctx, g, min_qdeg, asc, v.get()));
-    *out = v.get();
-    g->views[key] = std::move(v);
+    *out = v;
+    g->views[key] = v;
     if (built)
         *built = true;
     return BEEP_OK;

@@ -1,6 +1,7 @@
 // internal.h — shared host/device declarations of the B200 subgraph library.
 #pragma once
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstring>
@@ -123,7 +124,7 @@ struct Graph {
     uint32_t cutoff = 0;
     DevBuf row_ptr; // u32[n+1]
     DevBuf col;     // u32[m]
-    std::map<std::pair<int, int>, std::unique_ptr<View>> views;
+    std::map<std::pair<int, int>, std::shared_ptr<View>> views;
 };
 
 struct Query {
@@ -144,6 +145,24 @@ struct Ctx {
     DevBuf counter;      // u64 counters
     unsigned long long *h_pinned = nullptr; // pinned host mirror of small results
     uint64_t launches = 0; // kernels of this library launched on the context
+    cudaMemPool_t pool = nullptr; // stream-ordered pool for per-call buffers
+    // grow-only pinned host buffer for results read back by a call
+    unsigned long long *h_results = nullptr;
+    size_t h_results_n = 0;
+    beep_status host_results(size_t n, unsigned long long **out) {
+        if (n > h_results_n) {
+            if (h_results)
+                cudaFreeHost(h_results);
+            h_results = nullptr;
+            h_results_n = 0;
+            cudaError_t e = cudaMallocHost(&h_results, std::max<size_t>(n, 1024) * sizeof(unsigned long long));
+            if (e != cudaSuccess)
+                return fail(BEEP_ERR_OUT_OF_MEMORY, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+            h_results_n = std::max<size_t>(n, 1024);
+        }
+        *out = h_results;
+        return BEEP_OK;
+    }
 };
 
 // device entry points (device.cu)
@@ -151,8 +170,8 @@ beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m
                                         const uint32_t *d_col);
 beep_status graph_build_from_device_edges(Ctx *ctx, Graph *g, int64_t n_edges, const uint32_t *d_src,
                                           const uint32_t *d_dst);
-beep_status get_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, bool no_cache, View **out,
-                     bool *built, cudaEvent_t ev_begin);
+beep_status get_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, bool no_cache,
+                     std::shared_ptr<View> *out, bool *built);
 
 struct EnumRequest {
     uint64_t k = 0;
@@ -161,6 +180,28 @@ struct EnumRequest {
 
 beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t options, const EnumRequest *en,
                       beep_stats *stats);
+
+// One (graph, compiled query) of a multi-pair call.
+struct PairSpec {
+    Graph *g = nullptr;
+    QueryPlan plan;
+    const EnumRequest *en = nullptr;
+};
+// Count every pair in one set of launches; counts[i] receives pair i's count.
+beep_status run_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, beep_stats *stats,
+                      uint64_t *counts);
+
+// A planned multi-pair call: its launches and the buffers they use.
+struct LaunchPlan;
+struct LaunchPlanDeleter {
+    void operator()(LaunchPlan *p) const;
+};
+using LaunchPlanPtr = std::unique_ptr<LaunchPlan, LaunchPlanDeleter>;
+beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out);
+// Capture the plan's launches into a CUDA graph (relaunched by execute_plan).
+beep_status capture_plan(Ctx *ctx, LaunchPlan *lp);
+beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::vector<PairSpec> *specs,
+                         uint64_t *counts, size_t ncounts, beep_stats *stats);
 
 // host helpers (io.cpp)
 beep_status read_bel(const char *path, std::vector<uint32_t> &src, std::vector<uint32_t> &dst);

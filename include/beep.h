@@ -190,6 +190,28 @@ beep_status beep_count_ex(beep_ctx *ctx, beep_graph *g, const beep_query *q, bee
 beep_status beep_enumerate(beep_ctx *ctx, beep_graph *g, const beep_query *q, uint64_t k, int32_t *out_tuples,
                            uint64_t *n_out, uint64_t *total_count);
 
+/* ---- batched counting -------------------------------------------------- */
+
+/* Many (graph, query, mode) pairs counted by one set of launches: the roots
+ * of every pair are classified together, each kernel tier runs once over the
+ * roots of all pairs, and the launch sequence is captured into a CUDA graph
+ * on the first run and replayed afterwards. Replaces looping the plain count
+ * over the pairs (the reference runs one SG_Match per query and graph,
+ * subgraph_matching.cuh:178-231). The graphs and queries must outlive the
+ * batch; adding a pair after a run re-plans the batch. */
+typedef struct beep_batch beep_batch;
+enum {
+    /* Run the planned launches directly instead of through the CUDA graph. */
+    BEEP_OPT_NO_GRAPH = 1u << 4
+};
+beep_status beep_batch_create(beep_ctx *ctx, beep_batch **out);
+beep_status beep_batch_add(beep_batch *b, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t *index);
+/* counts[i] receives the count of the i-th added pair (array of at least
+ * beep_batch_size entries); stats (may be NULL) aggregates the run. */
+beep_status beep_batch_run(beep_batch *b, uint32_t options, uint64_t *counts, beep_stats *stats);
+beep_status beep_batch_size(const beep_batch *b, uint32_t *out);
+beep_status beep_batch_destroy(beep_batch *b);
+
 /* ---- counting without allocation --------------------------------------- */
 
 /* Size of the device scratch array the allocation-free path uses (64 MiB per
