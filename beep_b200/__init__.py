@@ -73,6 +73,23 @@ class PlanInfo(ctypes.Structure):
     ]
 
 
+class ServeOptions(ctypes.Structure):
+    _fields_ = [("max_batch", ctypes.c_uint32), ("streams", ctypes.c_uint32), ("hbm_reserve_bytes", ctypes.c_uint64),
+                ("count_options", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class ServeResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("K", ctypes.c_int32), ("count", ctypes.c_uint64),
+                ("n_tuples", ctypes.c_uint64), ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("matches", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("span_s", ctypes.c_double),
+                ("max_batch", ctypes.c_double)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("count", ctypes.c_uint64),
@@ -139,6 +156,14 @@ _SIGNATURES = [
     ("beep_batch_run", ctypes.c_int, [_vp, ctypes.c_uint32, _P(ctypes.c_uint64), _P(Stats)]),
     ("beep_batch_size", ctypes.c_int, [_vp, _P(ctypes.c_uint32)]),
     ("beep_batch_destroy", ctypes.c_int, [_vp]),
+    ("beep_serve_create", ctypes.c_int, [_vp, _P(ServeOptions), _P(_vp)]),
+    ("beep_serve_add_graph", ctypes.c_int, [_vp, _vp, _P(ctypes.c_int32)]),
+    ("beep_serve_submit", ctypes.c_int, [_vp, ctypes.c_int32, _vp, ctypes.c_int, ctypes.c_uint64,
+                                         _P(ctypes.c_uint64)]),
+    ("beep_serve_wait", ctypes.c_int, [_vp, ctypes.c_uint64, _P(ServeResult), _P(ctypes.c_int32), ctypes.c_uint64]),
+    ("beep_serve_drain", ctypes.c_int, [_vp]),
+    ("beep_serve_stats_get", ctypes.c_int, [_vp, _P(ServeStats)]),
+    ("beep_serve_destroy", ctypes.c_int, [_vp]),
     ("beep_count_noalloc", ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int64, _vp, _vp, _vp,
                                           ctypes.c_int, _P(ctypes.c_uint64)]),
     ("beep_gen_erdos_renyi", ctypes.c_int, [ctypes.c_int64, ctypes.c_double, ctypes.c_uint64, _P(ctypes.c_int64),
@@ -406,6 +431,65 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "_h", None):
             lib().beep_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request server over resident graphs with continuous batching."""
+
+    def __init__(self, ctx: Context, max_batch: int = 0, streams: int = 0, hbm_reserve_bytes: int = 0,
+                 count_options: int = 0):
+        opt = ServeOptions(max_batch, streams, hbm_reserve_bytes, count_options, 0)
+        h = _vp()
+        _check(lib().beep_serve_create(ctx.handle, ctypes.byref(opt), ctypes.byref(h)))
+        self._h = h
+        self.ctx = ctx
+        self._keep = []
+        self._queries = {}
+
+    def add_graph(self, graph: Graph) -> int:
+        gid = ctypes.c_int32()
+        _check(lib().beep_serve_add_graph(self._h, graph.handle, ctypes.byref(gid)))
+        self._keep.append(graph)
+        return int(gid.value)
+
+    def submit(self, graph_id: int, query, mode: int = SGM, k: int = 0) -> int:
+        q = query if isinstance(query, Query) else self._queries.setdefault(id(query), Query.from_edges(query))
+        rid = ctypes.c_uint64()
+        _check(lib().beep_serve_submit(self._h, int(graph_id), q.handle, int(mode), int(k), ctypes.byref(rid)))
+        return int(rid.value)
+
+    def wait(self, request_id: int, k: int = 0):
+        res = ServeResult()
+        buf = None
+        if k > 0:
+            buf = np.zeros((k, MAX_QUERY), dtype=np.int32)
+        st = lib().beep_serve_wait(self._h, int(request_id), ctypes.byref(res), _i32p(buf) if buf is not None else None,
+                                   int(k))
+        _check(st)
+        out = {"count": int(res.count), "latency_ms": res.latency_ms, "queue_ms": res.queue_ms, "K": res.K}
+        if buf is not None:
+            flat = buf.reshape(-1)[: int(res.n_tuples) * res.K]
+            out["tuples"] = flat.reshape(-1, res.K) if res.K else flat.reshape(0, 0)
+        return out
+
+    def drain(self) -> None:
+        _check(lib().beep_serve_drain(self._h))
+
+    def stats(self) -> dict:
+        st = ServeStats()
+        _check(lib().beep_serve_stats_get(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServeStats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().beep_serve_destroy(self._h)
             self._h = None
 
     def __del__(self):

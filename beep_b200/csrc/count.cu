@@ -61,6 +61,7 @@ struct EnumDev {
 struct Lp {
     uint32_t back[kMaxQ];
     uint32_t sym[kMaxQ];
+    int free_from;
 };
 
 __device__ __forceinline__ Lp load_lp(const DevPlan &pl) {
@@ -70,7 +71,55 @@ __device__ __forceinline__ Lp load_lp(const DevPlan &pl) {
         lp.back[i] = pl.back[i];
         lp.sym[i] = pl.sym[i];
     }
+    lp.free_from = pl.free_from;
     return lp;
+}
+
+// C(A, L) for L <= 4, exact through a 128-bit product (A < 2^32), reduced
+// mod 2^64 like every count here.
+__device__ __forceinline__ unsigned long long binom_le4(uint32_t A, int L) {
+    if (A < (uint32_t)L)
+        return 0ull;
+    unsigned __int128 num = 1;
+    for (int i = 0; i < L; ++i)
+        num *= (unsigned __int128)(A - (uint32_t)i);
+    const uint32_t fact = L <= 1 ? 1u : (L == 2 ? 2u : (L == 3 ? 6u : 24u));
+    return (unsigned long long)(num / fact);
+}
+
+// Positions P..DEND-1 form a free suffix (only the root as back edge, each
+// after the one before it): the number of ways to complete the assignment
+// x[1..P-1] is C(A, L) with L = DEND - P and A the unused domain vertices at
+// or above the first position's bound -- provided no later position has a
+// tighter bound from an assigned position. Returns false to fall back to the
+// enumeration.
+template <int P, int DEND>
+__device__ __forceinline__ bool free_suffix(const Lp &lp, uint32_t D, const uint32_t (&x)[kMaxQ],
+                                            unsigned long long &out) {
+    constexpr int L = DEND - P;
+    if constexpr (L > 4) {
+        return false;
+    } else {
+        if (P < lp.free_from)
+            return false;
+        uint32_t lo = 0;
+#pragma unroll
+        for (int q = 1; q < P; ++q)
+            if (lp.sym[P] >> q & 1u)
+                lo = max(lo, x[q] + 1);
+#pragma unroll
+        for (int p = P + 1; p < DEND; ++p)
+#pragma unroll
+            for (int q = 1; q < P; ++q)
+                if ((lp.sym[p] >> q & 1u) && x[q] + 1 > lo)
+                    return false;
+        uint32_t A = D > lo ? D - lo : 0u;
+#pragma unroll
+        for (int q = 1; q < P; ++q)
+            A -= (x[q] >= lo) ? 1u : 0u;
+        out = binom_le4(A, L);
+        return true;
+    }
 }
 
 // Domain of root r: list A = col[beg, beg + D); level-1 index starts at j0.
@@ -172,6 +221,13 @@ __device__ __forceinline__ void emit_bits(const EnumCtx &ec, const uint32_t (&x)
 template <int P, int DEND, bool ENUM>
 __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, uint64_t all, uint32_t (&x)[kMaxQ],
                                            unsigned long long &cnt, const EnumCtx &ec) {
+    if constexpr (!ENUM) {
+        unsigned long long f;
+        if (free_suffix<P, DEND>(lp, (uint32_t)__popcll(all), x, f)) {
+            cnt += f;
+            return;
+        }
+    }
     uint64_t c = all;
     const uint32_t bk = lp.back[P], sy = lp.sym[P];
 #pragma unroll
@@ -202,6 +258,14 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
 template <int P, int DEND, bool ENUM>
 __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint32_t W, uint32_t D,
                                          uint32_t (&x)[kMaxQ], unsigned long long &cnt, int lane, const EnumCtx &ec) {
+    if constexpr (!ENUM) {
+        unsigned long long f;
+        if (free_suffix<P, DEND>(lp, D, x, f)) { // warp-uniform
+            if (lane == 0)
+                cnt += f;
+            return;
+        }
+    }
     const uint32_t bk = lp.back[P], sy = lp.sym[P];
     uint32_t lo = 0;
 #pragma unroll
@@ -1453,6 +1517,34 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
     if (stats)
         *stats = st;
     return BEEP_OK;
+}
+
+beep_status launch_plan_async(Ctx *ctx, LaunchPlan *lp) {
+    if (!lp->own_h_counts) {
+        unsigned long long *h = nullptr;
+        BEEP_CUDA_TRY(cudaMallocHost(&h, (lp->np + 4) * sizeof(unsigned long long)));
+        lp->h_counts = h;
+        lp->own_h_counts = true;
+    }
+    beep_stats st;
+    std::memset(&st, 0, sizeof(st));
+    BEEP_TRY(issue(ctx, lp, false, st, nullptr, nullptr));
+    BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, (lp->np + 4) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    return BEEP_OK;
+}
+
+uint64_t plan_count(const LaunchPlan *lp, size_t spec_index) {
+    for (uint32_t i = 0; i < lp->np; ++i)
+        if (lp->live[i] == spec_index)
+            return lp->h_counts[i];
+    return 0;
+}
+
+int plan_launches(const LaunchPlan *lp) {
+    int n = lp->st.kernel_launches;
+    for (auto &r : lp->recs)
+        n += r.kind != LaunchRec::kMemset;
+    return n;
 }
 
 beep_status run_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, beep_stats *stats,

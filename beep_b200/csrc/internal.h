@@ -54,7 +54,7 @@ struct DevPlan {
     int32_t pos1_after_root; // position 1 must follow the root in the priority order
     int32_t restricted;      // every position follows the root: search only the out-list
     int32_t asc;             // ascending (degree, id) priority order
-    int32_t pad;
+    int32_t free_from;       // positions [free_from, dend) touch only the root and form a symmetry chain
 };
 
 struct QueryPlan {
@@ -202,6 +202,12 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
 beep_status capture_plan(Ctx *ctx, LaunchPlan *lp);
 beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::vector<PairSpec> *specs,
                          uint64_t *counts, size_t ncounts, beep_stats *stats);
+// Issue the plan and its count read-back on ctx->stream without waiting.
+beep_status launch_plan_async(Ctx *ctx, LaunchPlan *lp);
+// After the stream passed the launch: the count of the spec_index-th pair.
+uint64_t plan_count(const LaunchPlan *lp, size_t spec_index);
+// Kernel launches of planning plus one execution.
+int plan_launches(const LaunchPlan *lp);
 
 // host helpers (io.cpp)
 beep_status read_bel(const char *path, std::vector<uint32_t> &src, std::vector<uint32_t> &dst);

@@ -38,6 +38,8 @@ WORKLOADS = {
            "graph": ("rmat", (20, 3, 0.57, 0.19, 0.19, 7)), "patterns": ["k4", "diamond"], "mode": "sgm"},
     "c1": {"desc": "plain-small: ER G(4096, 0.004) seed 1; triangle (sgc)",
            "graph": ("er", (4096, 0.004, 1)), "patterns": ["triangle"], "mode": "sgc"},
+    "c4": {"desc": "batched: Chung-Lu graphs (exponent 2.1, seed 13) x the 15 central 4-5-vertex patterns (sgm)"},
+    "c5": {"desc": "served: Poisson requests (seed 17) over resident Chung-Lu graphs (exponent 2.1)"},
 }
 
 
@@ -256,6 +258,149 @@ def reference_arm(args, wl):
 
 
 # ---------------------------------------------------------------------------
+# batched and served forms
+# ---------------------------------------------------------------------------
+def c4_graph_specs(n_graphs, lo_scale, hi_scale, dmin, dmax, seed=13):
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_graphs):
+        n = int(round(2 ** rng.uniform(lo_scale, hi_scale)))
+        d = float(rng.uniform(dmin, dmax))
+        specs.append((n, d, 2.1, seed * 1000 + i))
+    return specs
+
+
+def bench_batched(args):
+    import numpy as np
+    import torch
+
+    import beep_b200 as B
+    from beep_b200 import patterns as P
+
+    specs = c4_graph_specs(args.c4_graphs, 10, args.c4_max_scale, 8, args.c4_max_degree)
+    ctx = B.Context(0)
+    t0 = time.perf_counter()
+    host = [B.gen_chung_lu(*sp) for sp in specs]
+    gen_s = time.perf_counter() - t0
+    graphs = [B.Graph.from_csr(ctx, rp, col) for rp, col in host]
+    pats = [B.Query.from_edges(q) for q in P.central_patterns(4) + P.central_patterns(5)]
+    pairs = [(g, q) for g in graphs for q in pats]
+    # plain loop: one count per pair (views cached on the graphs after the first pass)
+    for g, q in pairs:
+        B.count(g, q)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain_total = 0
+    for g, q in pairs:
+        plain_total += B.count(g, q)
+    plain_s = time.perf_counter() - t0
+    batch = B.Batch(ctx)
+    for g, q in pairs:
+        batch.add(g, q)
+    t0 = time.perf_counter()
+    first = batch.run()  # plans and captures
+    plan_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        batch.run()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        got = batch.run()
+        times.append(time.perf_counter() - t0)
+    assert got == first and sum(got) == plain_total, "batched counts differ from the plain loop"
+    step_s = statistics.median(times)
+    line = {"metric": METRIC, "impl": "ours", "form": "batched", "value": sum(got) / step_s, "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOADS["c4"]["desc"], "graphs": len(graphs), "patterns": len(pats),
+                       "pairs": len(pairs), "n_log2_range": [10, args.c4_max_scale],
+                       "avg_degree_range": [8, args.c4_max_degree],
+                       "edges_directed": int(sum(len(c) for _, c in host)), "matches_per_step": int(sum(got)),
+                       "step": "one replay of the captured CUDA graph over every pair (views resident)"},
+            "plain_loop": {"value": plain_total / plain_s, "ms": plain_s * 1e3,
+                           "what": "beep_count per pair, same pairs, views resident"},
+            "speedup_vs_plain_loop": plain_s / step_s, "plan_and_capture_ms": plan_s * 1e3,
+            "generate_s": gen_s}
+    print(json.dumps(line), flush=True)
+    batch.close()
+    for g in graphs:
+        g.close()
+    ctx.close()
+
+
+def bench_served(args):
+    import numpy as np
+    import torch
+
+    import beep_b200 as B
+    from beep_b200 import patterns as P
+
+    rng = np.random.default_rng(17)
+    ctx = B.Context(0)
+    graphs, host = [], []
+    for i in range(args.c5_graphs):
+        m_und = 10 ** rng.uniform(4, args.c5_max_log10_edges)
+        n = max(64, int(2 * m_und / 16))
+        rp, col = B.gen_chung_lu(n, 16.0, 2.1, 17000 + i)
+        host.append((rp, col))
+        graphs.append(B.Graph.from_csr(ctx, rp, col))
+    names = ["triangle", "diamond", "k4", "tailed_triangle", "w5", "k5"]
+    queries = {nm: B.Query.from_edges(P.NAMED[nm]) for nm in names}
+    n_req = int(args.c5_rate * args.c5_seconds)
+    gaps = rng.exponential(1.0 / args.c5_rate, size=n_req)
+    arrivals = np.cumsum(gaps)
+    reqs = [(int(rng.integers(0, len(graphs))), names[int(rng.integers(0, len(names)))],
+             args.c5_k if rng.random() < 0.2 else 0) for _ in range(n_req)]
+    # serial plain execution of the same requests (views warmed first)
+    for g in graphs:
+        for nm in names:
+            B.count(g, queries[nm])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    serial_matches = 0
+    for gi, nm, k in reqs:
+        if k:
+            _, tot = B.enumerate_matches(graphs[gi], queries[nm], k)
+            serial_matches += tot
+        else:
+            serial_matches += B.count(graphs[gi], queries[nm])
+    serial_s = time.perf_counter() - t0
+    srv = B.Server(ctx, max_batch=args.c5_max_batch, streams=args.c5_streams)
+    gids = [srv.add_graph(g) for g in graphs]
+    start = time.perf_counter()
+    rids = []
+    for (gi, nm, k), at in zip(reqs, arrivals):
+        now = time.perf_counter() - start
+        if at > now:
+            time.sleep(at - now)
+        rids.append((srv.submit(gids[gi], queries[nm], B.SGM, k), k))
+    served_matches = 0
+    for rid, k in rids:
+        served_matches += srv.wait(rid, k)["count"]
+    st = srv.stats()
+    assert served_matches == serial_matches, "served counts differ from the serial run"
+    line = {"metric": METRIC, "impl": "ours", "form": "served", "value": served_matches / st["span_s"],
+            "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
+            "config": {"workload": WORKLOADS["c5"]["desc"], "graphs": len(graphs),
+                       "log10_undirected_edges_range": [4, args.c5_max_log10_edges], "avg_degree": 16,
+                       "rate_per_s": args.c5_rate, "requests": n_req, "enumerate_fraction": 0.2,
+                       "enumerate_k": args.c5_k, "patterns": names, "max_batch": args.c5_max_batch,
+                       "streams": args.c5_streams},
+            "serial_plain": {"value": serial_matches / serial_s, "s": serial_s},
+            "speedup_vs_serial_plain": (served_matches / st["span_s"]) / (serial_matches / serial_s),
+            "batches": st["batches"], "largest_batch": st["max_batch"], "span_s": st["span_s"],
+            "offered_span_s": float(arrivals[-1]) if n_req else 0.0}
+    print(json.dumps(line), flush=True)
+    srv.close()
+    for g in graphs:
+        g.close()
+    ctx.close()
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def main():
@@ -268,8 +413,24 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-port", action="store_true", help="reference arm: use the CPU port")
     ap.add_argument("--reference-timeout", type=float, default=300.0)
+    ap.add_argument("--c4-graphs", type=int, default=256)
+    ap.add_argument("--c4-max-scale", type=float, default=18.0)
+    ap.add_argument("--c4-max-degree", type=float, default=64.0)
+    ap.add_argument("--c5-graphs", type=int, default=32)
+    ap.add_argument("--c5-max-log10-edges", type=float, default=7.0)
+    ap.add_argument("--c5-rate", type=float, default=2000.0)
+    ap.add_argument("--c5-seconds", type=float, default=2.0)
+    ap.add_argument("--c5-k", type=int, default=10000)
+    ap.add_argument("--c5-max-batch", type=int, default=64)
+    ap.add_argument("--c5-streams", type=int, default=4)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
+    if args.workload == "c4":
+        bench_batched(args)
+        return
+    if args.workload == "c5":
+        bench_served(args)
+        return
     if args.impl == "reference":
         reference_arm(args, wl)
         return

@@ -212,6 +212,53 @@ beep_status beep_batch_run(beep_batch *b, uint32_t options, uint64_t *counts, be
 beep_status beep_batch_size(const beep_batch *b, uint32_t *out);
 beep_status beep_batch_destroy(beep_batch *b);
 
+/* ---- serving ------------------------------------------------------------ */
+
+/* A request server over resident graphs with continuous batching. Requests
+ * are queued by beep_serve_submit and return at once; a scheduler thread
+ * admits them while the free HBM stays above a reserve, plans whatever has
+ * arrived as one multi-pair call and launches it on one of several streams
+ * without waiting, so batches overlap on the device and requests arriving
+ * meanwhile join the next batch as soon as a stream frees up. The reference
+ * has no counterpart: it runs one SG_Match per query and graph
+ * (subgraph_matching.cuh:178-231). Graphs added to a server must outlive it
+ * and must not be used by other calls while it runs. */
+typedef struct beep_server beep_server;
+typedef struct beep_serve_options {
+    uint32_t max_batch;         /* requests per batch (0: 64) */
+    uint32_t streams;           /* batches in flight (0: 4) */
+    uint64_t hbm_reserve_bytes; /* free HBM the admission keeps (0: 1 GiB) */
+    uint32_t count_options;     /* BEEP_OPT_REFERENCE_ROOT_CAP or 0 */
+    uint32_t reserved;
+} beep_serve_options;
+typedef struct beep_serve_result {
+    beep_status status;
+    int32_t K;                  /* query vertices (tuple width) */
+    uint64_t count;             /* exact number of matches */
+    uint64_t n_tuples;          /* tuples returned (first-k requests) */
+    double latency_ms;          /* arrival to completion */
+    double queue_ms;            /* arrival to launch of its batch */
+} beep_serve_result;
+typedef struct beep_serve_stats {
+    uint64_t requests, batches, matches, kernel_launches;
+    double p50_ms, p99_ms, mean_ms, max_ms;
+    double span_s;              /* first arrival to last completion */
+    double max_batch;
+} beep_serve_stats;
+beep_status beep_serve_create(beep_ctx *ctx, const beep_serve_options *opt, beep_server **out);
+beep_status beep_serve_add_graph(beep_server *s, beep_graph *g, int32_t *graph_id);
+/* k = 0: count (mode sgm or sgc); k > 0: also return the first k matches
+ * (sgm semantics). */
+beep_status beep_serve_submit(beep_server *s, int32_t graph_id, const beep_query *q, beep_mode mode, uint64_t k,
+                              uint64_t *request_id);
+/* Blocks until the request is done; consumes it. tuples (may be NULL) gets
+ * up to tuples_cap tuples of K int32 in original query-vertex order. */
+beep_status beep_serve_wait(beep_server *s, uint64_t request_id, beep_serve_result *res, int32_t *tuples,
+                            uint64_t tuples_cap);
+beep_status beep_serve_drain(beep_server *s);
+beep_status beep_serve_stats_get(beep_server *s, beep_serve_stats *out);
+beep_status beep_serve_destroy(beep_server *s);
+
 /* ---- counting without allocation --------------------------------------- */
 
 /* Size of the device scratch array the allocation-free path uses (64 MiB per

@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 def graphs():
     return [
         B.gen_chung_lu(1 << 10, 8.0, 2.1, 13),
-        B.gen_chung_lu(1 << 12, 16.0, 2.1, 14),
+        B.gen_chung_lu(1 << 11, 10.0, 2.1, 14),
         B.gen_rmat(11, 8, 0.57, 0.19, 0.19, 3),
         B.gen_erdos_renyi(600, 0.03, 4),
     ]
