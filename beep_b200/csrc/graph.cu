@@ -23,22 +23,45 @@ constexpr unsigned kFull = 0xffffffffu;
 
 __global__ void k_check_csr(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n, int64_t m,
                             unsigned *bad) {
+    // Lane l checks vertex base + l alone when its row has <= 32 entries;
+    // longer rows are checked by the whole warp afterwards.
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
-        const uint32_t b = rp[v], e = rp[v + 1];
-        if (e < b || e > m) {
-            if (lane == 0)
-                atomicOr(bad, 2u); // row pointers unusable
-            continue;
+    unsigned flag = 0;
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += warps * 32) {
+        const int64_t v = base + lane;
+        bool big = false;
+        uint32_t b = 0, e = 0;
+        if (v < n) {
+            b = rp[v];
+            e = rp[v + 1];
+            if (e < b || e > m)
+                flag |= 2u; // row pointers unusable
+            else if (e - b > 32)
+                big = true;
+            else
+                for (uint32_t i = b; i < e; ++i) {
+                    const uint32_t w = col[i];
+                    if (!(w < n && w != (uint32_t)v && (i == b || col[i - 1] < w)))
+                        flag |= 1u;
+                }
         }
-        for (uint32_t i = b + lane; i < e; i += 32) {
-            const uint32_t w = col[i];
-            bool ok = w < n && w != (uint32_t)v && (i == b || col[i - 1] < w);
-            if (!ok)
-                atomicOr(bad, 1u);
+        unsigned mask = __ballot_sync(kFull, big);
+        while (mask) {
+            const int L = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const uint32_t u = (uint32_t)(base + L);
+            const uint32_t ub = __shfl_sync(kFull, b, L), ue = __shfl_sync(kFull, e, L);
+            for (uint32_t i = ub + lane; i < ue; i += 32) {
+                const uint32_t w = col[i];
+                if (!(w < n && w != u && (i == ub || col[i - 1] < w)))
+                    flag |= 1u;
+            }
         }
     }
+    flag = __reduce_or_sync(kFull, flag);
+    if (lane == 0 && flag)
+        atomicOr(bad, flag);
 }
 
 __global__ void k_csr_keys(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n,
@@ -128,21 +151,41 @@ __global__ void k_peel_mark(const uint32_t *__restrict__ deg, uint8_t *alive, in
 // common_utils.cuh:99-133, 217-246).
 __global__ void k_peel_degree(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
                               const uint8_t *__restrict__ alive, int64_t n, uint32_t *deg) {
+    // lane-serial for rows of <= 32 entries, warp-cooperative for longer ones
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
-        if (!alive[v]) {
-            if (lane == 0)
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += warps * 32) {
+        const int64_t v = base + lane;
+        bool big = false;
+        uint32_t b = 0, e = 0;
+        if (v < n) {
+            if (!alive[v]) {
                 deg[v] = 0;
-            continue;
+            } else {
+                b = rp[v];
+                e = rp[v + 1];
+                if (e - b > 32) {
+                    big = true;
+                } else {
+                    uint32_t c = 0;
+                    for (uint32_t i = b; i < e; ++i)
+                        c += alive[col[i]];
+                    deg[v] = c;
+                }
+            }
         }
-        const uint32_t b = rp[v], e = rp[v + 1];
-        uint32_t c = 0;
-        for (uint32_t i = b + lane; i < e; i += 32)
-            c += alive[col[i]];
-        c = __reduce_add_sync(kFull, c);
-        if (lane == 0)
-            deg[v] = c;
+        unsigned mask = __ballot_sync(kFull, big);
+        while (mask) {
+            const int L = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const uint32_t ub = __shfl_sync(kFull, b, L), ue = __shfl_sync(kFull, e, L);
+            uint32_t c = 0;
+            for (uint32_t i = ub + lane; i < ue; i += 32)
+                c += alive[col[i]];
+            c = __reduce_add_sync(kFull, c);
+            if (lane == 0)
+                deg[base + L] = c;
+        }
     }
 }
 
@@ -187,22 +230,47 @@ __global__ void k_rank(const uint64_t *__restrict__ keys, int64_t n_alive, uint3
 __global__ void k_fill_rows(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
                             const uint32_t *__restrict__ orig, const uint32_t *__restrict__ rank,
                             const uint32_t *__restrict__ new_rp, int64_t n_alive, uint32_t *new_col) {
+    // lane-serial for rows of <= 32 entries, warp-cooperative (ballot
+    // compaction) for longer ones
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_alive; i += warps) {
-        const uint32_t v = orig[i];
-        const uint32_t b = rp[v], e = rp[v + 1];
-        uint32_t out = new_rp[i];
-        for (uint32_t base = b; base < e; base += 32) {
-            const uint32_t idx = base + lane;
-            uint32_t r = 0xffffffffu;
-            if (idx < e)
-                r = rank[col[idx]];
-            const bool keep = r != 0xffffffffu;
-            const unsigned bal = __ballot_sync(kFull, keep);
-            if (keep)
-                new_col[out + __popc(bal & ((1u << lane) - 1u))] = r;
-            out += __popc(bal);
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n_alive;
+         base += warps * 32) {
+        const int64_t i = base + lane;
+        bool big = false;
+        uint32_t b = 0, e = 0, out = 0;
+        if (i < n_alive) {
+            const uint32_t v = orig[i];
+            b = rp[v];
+            e = rp[v + 1];
+            out = new_rp[i];
+            if (e - b > 32) {
+                big = true;
+            } else {
+                for (uint32_t k = b; k < e; ++k) {
+                    const uint32_t r = rank[col[k]];
+                    if (r != 0xffffffffu)
+                        new_col[out++] = r;
+                }
+            }
+        }
+        unsigned mask = __ballot_sync(kFull, big);
+        while (mask) {
+            const int L = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const uint32_t ub = __shfl_sync(kFull, b, L), ue = __shfl_sync(kFull, e, L);
+            uint32_t o = __shfl_sync(kFull, out, L);
+            for (uint32_t k0 = ub; k0 < ue; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                uint32_t r = 0xffffffffu;
+                if (k < ue)
+                    r = rank[col[k]];
+                const bool keep = r != 0xffffffffu;
+                const unsigned bal = __ballot_sync(kFull, keep);
+                if (keep)
+                    new_col[o + __popc(bal & ((1u << lane) - 1u))] = r;
+                o += __popc(bal);
+            }
         }
     }
 }
@@ -339,7 +407,7 @@ beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m
     unsigned *d_bad = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 32);
     BEEP_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 4, s));
     if (n > 0)
-        k_check_csr<<<grid_for(n * 32, 256, ctx->num_sms), 256, 0, s>>>(d_rp, d_col, n, m, d_bad);
+        k_check_csr<<<grid_for(n, 256, ctx->num_sms), 256, 0, s>>>(d_rp, d_col, n, m, d_bad);
         ++ctx->launches;
     BEEP_CUDA_TRY(cudaGetLastError());
     unsigned h_bad = 0;
@@ -435,7 +503,6 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     unsigned long long *d_removed = ctx->counter.as<unsigned long long>();
 
     const int gv = grid_for(n, 256, ctx->num_sms);
-    const int gw = grid_for(n * 32, 256, ctx->num_sms);
     if (n > 0)
         k_peel_init<<<gv, 256, 0, s>>>(rp, n, deg, alive);
         ++ctx->launches;
@@ -454,7 +521,7 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
             BEEP_CUDA_TRY(cudaStreamSynchronize(s));
             removed = ctx->h_pinned[0];
             if (removed > 0)
-                k_peel_degree<<<gw, 256, 0, s>>>(rp, col, alive, n, deg);
+                k_peel_degree<<<gv, 256, 0, s>>>(rp, col, alive, n, deg);
                 ++ctx->launches;
             BEEP_CUDA_TRY(cudaGetLastError());
         }
@@ -504,7 +571,7 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     v->m = h_m;
     BEEP_TRY(v->col.reserve((size_t)(h_m > 0 ? h_m : 1) * 4));
     if (na > 0)
-        k_fill_rows<<<grid_for(na * 32, 256, ctx->num_sms), 256, 0, s>>>(rp, col, v->orig.as<uint32_t>(), rank,
+        k_fill_rows<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(rp, col, v->orig.as<uint32_t>(), rank,
                                                                            nrp, na, col_tmp);
     BEEP_CUDA_TRY(cudaGetLastError());
     if (h_m > 0) {

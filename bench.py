@@ -136,15 +136,35 @@ def dist_setup():
     return world, rank, local
 
 
+def _coll_device():
+    import torch
+    import torch.distributed as dist
+
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def max_over_ranks(x: float, world: int) -> float:
+    """Largest value over the ranks (device times are reported as the max)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_coll_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def sum_over_ranks(x: int, world: int) -> int:
+    """Sum of an exact count over the ranks (int64 all-reduce)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.int64, device=_coll_device())
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(t.item())
 
 
 def barrier(world: int):
@@ -509,6 +529,19 @@ def main():
     e_ms = max_over_ranks(e_ms, world)
     e2e_value = world * (e_total // args.steps) / (e_ms / args.steps / 1e3)
 
+    # wall-clock of each public call in one untimed step (the calls return after their device work)
+    host_ms = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g = B.Graph.from_device_csr(ctx, n, m, d_rp.data_ptr(), d_col.data_ptr())
+    host_ms["graph_from_device_csr"] = (time.perf_counter() - t0) * 1e3
+    for name, q in zip(wl["patterns"], queries):
+        t0 = time.perf_counter()
+        B.count(g, q, mode, 0, ctx=ctx)
+        host_ms[f"count_{name}"] = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    g.close()
+    host_ms["graph_destroy"] = (time.perf_counter() - t0) * 1e3
     # adjacency bytes per tier, from one untimed pass (identical every step)
     _, byte_sts = step(False, B.OPT_ALG_BYTES)
     for sts in allst:
@@ -547,6 +580,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * (n + 1) + 4 * m),
                 "d2h_bytes_per_step": 8 * len(queries) + 16, "ms_per_step": e_ms / args.steps},
         "gpu_launches": int(launches),
+        "host_calls_ms": host_ms,
         "phases_ms_per_step": {"prep": prep_ms / args.steps, "count": count_ms / args.steps,
                                **{k: v[0] / args.steps for k, v in agg.items()}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
