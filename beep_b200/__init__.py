@@ -149,6 +149,8 @@ _SIGNATURES = [
     ("beep_query_plan", ctypes.c_int, [_vp, ctypes.c_int, _P(PlanInfo)]),
     ("beep_count", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _P(ctypes.c_uint64)]),
     ("beep_count_ex", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_uint32, _P(Stats)]),
+    ("beep_count_shard", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_uint32, _P(Stats)]),
     ("beep_enumerate", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _P(ctypes.c_int32), _P(ctypes.c_uint64),
                                       _P(ctypes.c_uint64)]),
     ("beep_batch_create", ctypes.c_int, [_vp, _P(_vp)]),
@@ -508,6 +510,16 @@ def count_noalloc(device: int, n: int, m: int, d_row_ptr: int, d_col_ind: int, q
     _check(lib().beep_count_noalloc(int(device), _vp(cuda_stream) if cuda_stream else None, int(n), int(m),
                                     _vp(d_row_ptr), _vp(d_col_ind), q.handle, int(mode), ctypes.byref(out)))
     return int(out.value)
+
+
+def count_shard(graph: Graph, query, shard: int, nshards: int, mode: int = SGM, options: int = 0,
+                ctx: Context | None = None) -> int:
+    """Count of the roots whose input vertex id % nshards == shard."""
+    q = _as_query(query)
+    st = Stats()
+    _check(lib().beep_count_shard(ctx.handle if ctx else None, graph.handle, q.handle, int(mode), int(options),
+                                  int(shard), int(nshards), ctypes.byref(st)))
+    return int(st.count)
 
 
 def enumerate_matches(graph: Graph, query, k: int, ctx: Context | None = None):

@@ -138,6 +138,7 @@ void ctx_free(beep_ctx *ctx) {
         cudaFreeHost(ctx->impl.h_pinned);
     if (ctx->impl.h_results)
         cudaFreeHost(ctx->impl.h_results);
+    ctx->impl.release_side();
     if (ctx->impl.pool)
         cudaMemPoolDestroy(ctx->impl.pool);
     if (ctx->impl.own_stream)
@@ -346,6 +347,27 @@ beep_status beep_count_ex(beep_ctx *ctx, beep_graph *g, const beep_query *q, bee
     BEEP_TRY(compile_plan(q->impl.qn, q->impl.row_ptr, q->impl.col, mode, &p));
     beep_stats st;
     BEEP_TRY(run_count(&ctx->impl, &g->impl, p, options, nullptr, &st));
+    ctx->impl.launches += (uint64_t)st.kernel_launches;
+    if (stats)
+        *stats = st;
+    return BEEP_OK;
+}
+
+beep_status beep_count_shard(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t options,
+                             uint32_t shard, uint32_t nshards, beep_stats *stats) {
+    if (!g || !q || nshards == 0 || shard >= nshards)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_count_shard: bad arguments");
+    if (mode != BEEP_MODE_SGM && mode != BEEP_MODE_SGC)
+        return fail(BEEP_ERR_INVALID_ARG, "unknown mode");
+    if (!ctx)
+        ctx = g->ctx;
+    if (ctx->impl.device != g->impl.device)
+        return fail(BEEP_ERR_INVALID_ARG, "graph lives on another device");
+    BEEP_TRY(bind(ctx));
+    QueryPlan p;
+    BEEP_TRY(compile_plan(q->impl.qn, q->impl.row_ptr, q->impl.col, mode, &p));
+    beep_stats st;
+    BEEP_TRY(run_count(&ctx->impl, &g->impl, p, options, nullptr, &st, shard, nshards));
     ctx->impl.launches += (uint64_t)st.kernel_launches;
     if (stats)
         *stats = st;

