@@ -62,6 +62,7 @@ struct Lp {
     uint32_t back[kMaxQ];
     uint32_t sym[kMaxQ];
     int free_from;
+    uint32_t free_back;
 };
 
 __device__ __forceinline__ Lp load_lp(const DevPlan &pl) {
@@ -72,6 +73,7 @@ __device__ __forceinline__ Lp load_lp(const DevPlan &pl) {
         lp.sym[i] = pl.sym[i];
     }
     lp.free_from = pl.free_from;
+    lp.free_back = pl.free_back;
     return lp;
 }
 
@@ -87,39 +89,48 @@ __device__ __forceinline__ unsigned long long binom_le4(uint32_t A, int L) {
     return (unsigned long long)(num / fact);
 }
 
-// Positions P..DEND-1 form a free suffix (only the root as back edge, each
-// after the one before it): the number of ways to complete the assignment
-// x[1..P-1] is C(A, L) with L = DEND - P and A the unused domain vertices at
-// or above the first position's bound -- provided no later position has a
-// tighter bound from an assigned position. Returns false to fall back to the
-// enumeration.
+// Positions P..DEND-1 form a free suffix when they share one back-edge set B
+// (none of it inside the suffix) and each must follow the one before it: the
+// completions of an assignment x[1..P-1] are then the L-subsets (L = DEND - P)
+// of position P's candidate set -- provided no later position has a tighter
+// bound from an assigned position than position P has (checked here), so the
+// count is C(A, L) with A = |candidates of P|. With B empty, A is the unused
+// domain vertices at or above P's bound and needs no bitmap.
 template <int P, int DEND>
-__device__ __forceinline__ bool free_suffix(const Lp &lp, uint32_t D, const uint32_t (&x)[kMaxQ],
-                                            unsigned long long &out) {
+__device__ __forceinline__ bool suffix_applies(const Lp &lp, const uint32_t (&x)[kMaxQ], uint32_t lo) {
     constexpr int L = DEND - P;
     if constexpr (L > 4) {
         return false;
     } else {
         if (P < lp.free_from)
             return false;
-        uint32_t lo = 0;
-#pragma unroll
-        for (int q = 1; q < P; ++q)
-            if (lp.sym[P] >> q & 1u)
-                lo = max(lo, x[q] + 1);
 #pragma unroll
         for (int p = P + 1; p < DEND; ++p)
 #pragma unroll
             for (int q = 1; q < P; ++q)
                 if ((lp.sym[p] >> q & 1u) && x[q] + 1 > lo)
                     return false;
-        uint32_t A = D > lo ? D - lo : 0u;
-#pragma unroll
-        for (int q = 1; q < P; ++q)
-            A -= (x[q] >= lo) ? 1u : 0u;
-        out = binom_le4(A, L);
         return true;
     }
+}
+
+template <int P>
+__device__ __forceinline__ uint32_t level_bound(const Lp &lp, const uint32_t (&x)[kMaxQ]) {
+    uint32_t lo = 0;
+#pragma unroll
+    for (int q = 1; q < P; ++q)
+        if (lp.sym[P] >> q & 1u)
+            lo = max(lo, x[q] + 1);
+    return lo;
+}
+
+template <int P>
+__device__ __forceinline__ uint32_t free_count_rootonly(uint32_t D, const uint32_t (&x)[kMaxQ], uint32_t lo) {
+    uint32_t A = D > lo ? D - lo : 0u;
+#pragma unroll
+    for (int q = 1; q < P; ++q)
+        A -= (x[q] >= lo) ? 1u : 0u;
+    return A;
 }
 
 // Domain of root r: list A = col[beg, beg + D); level-1 index starts at j0.
@@ -221,11 +232,15 @@ __device__ __forceinline__ void emit_bits(const EnumCtx &ec, const uint32_t (&x)
 template <int P, int DEND, bool ENUM>
 __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, uint64_t all, uint32_t (&x)[kMaxQ],
                                            unsigned long long &cnt, const EnumCtx &ec) {
-    if constexpr (!ENUM) {
-        unsigned long long f;
-        if (free_suffix<P, DEND>(lp, (uint32_t)__popcll(all), x, f)) {
-            cnt += f;
-            return;
+    bool closed = false; // count this level's candidates as C(A, DEND - P)
+    if constexpr (!ENUM && DEND - P <= 4) {
+        const uint32_t lo = level_bound<P>(lp, x);
+        if (suffix_applies<P, DEND>(lp, x, lo)) {
+            if (lp.free_back == 0) {
+                cnt += binom_le4(free_count_rootonly<P>((uint32_t)__popcll(all), x, lo), DEND - P);
+                return;
+            }
+            closed = true;
         }
     }
     uint64_t c = all;
@@ -237,6 +252,10 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
         c &= ~(1ull << x[q]);
         if (sy >> q & 1u)
             c &= ~((2ull << x[q]) - 1ull); // keep bits above x[q]
+    }
+    if (closed) {
+        cnt += binom_le4((uint32_t)__popcll(c), DEND - P);
+        return;
     }
     if constexpr (P == DEND - 1) {
         if constexpr (ENUM)
@@ -258,20 +277,20 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
 template <int P, int DEND, bool ENUM>
 __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint32_t W, uint32_t D,
                                          uint32_t (&x)[kMaxQ], unsigned long long &cnt, int lane, const EnumCtx &ec) {
-    if constexpr (!ENUM) {
-        unsigned long long f;
-        if (free_suffix<P, DEND>(lp, D, x, f)) { // warp-uniform
-            if (lane == 0)
-                cnt += f;
-            return;
+    const uint32_t bk = lp.back[P];
+    const uint32_t lo = level_bound<P>(lp, x);
+    bool closed = false; // warp-uniform: count this level's candidates as C(A, DEND - P)
+    if constexpr (!ENUM && DEND - P <= 4) {
+        if (suffix_applies<P, DEND>(lp, x, lo)) {
+            if (lp.free_back == 0) {
+                if (lane == 0)
+                    cnt += binom_le4(free_count_rootonly<P>(D, x, lo), DEND - P);
+                return;
+            }
+            closed = true;
         }
     }
-    const uint32_t bk = lp.back[P], sy = lp.sym[P];
-    uint32_t lo = 0;
-#pragma unroll
-    for (int q = 1; q < P; ++q)
-        if (sy >> q & 1u)
-            lo = max(lo, x[q] + 1);
+    uint32_t acc = 0;
     const uint32_t nch = (W + 31) >> 5;
     const uint32_t tail = D & 31;
     for (uint32_t ch = lo >> 10; ch < nch; ++ch) {
@@ -292,6 +311,10 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
             else if (lw == k)
                 w &= ~((1u << (lo & 31)) - 1u);
         }
+        if (closed) {
+            acc += (uint32_t)__popc(w);
+            continue;
+        }
         if constexpr (P == DEND - 1) {
             if constexpr (ENUM)
                 emit_bits(ec, x, P, (uint64_t)w, k << 5);
@@ -309,6 +332,11 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
                 bal = __ballot_sync(kFull, w != 0);
             }
         }
+    }
+    if (closed) {
+        const uint32_t A = __reduce_add_sync(kFull, acc);
+        if (lane == 0)
+            cnt += binom_le4(A, DEND - P);
     }
 }
 

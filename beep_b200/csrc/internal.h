@@ -54,7 +54,9 @@ struct DevPlan {
     int32_t pos1_after_root; // position 1 must follow the root in the priority order
     int32_t restricted;      // every position follows the root: search only the out-list
     int32_t asc;             // ascending (degree, id) priority order
-    int32_t free_from;       // positions [free_from, dend) touch only the root and form a symmetry chain
+    int32_t free_from;       // positions [free_from, dend) share one back-edge set and form a symmetry chain
+    uint32_t free_back;      // that back-edge set (bits q >= 1; 0: only the root)
+    int32_t pad2;
 };
 
 struct QueryPlan {

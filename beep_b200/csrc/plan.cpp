@@ -239,16 +239,21 @@ beep_status compile_plan(int32_t qn, const std::vector<int32_t> &rp, const std::
     }
     D.restricted = restricted ? 1 : 0;
     P.restricted = D.restricted;
-    // Free suffix: the last positions whose only back edge is the root and
-    // where each follows the one before it. Their completions are counted in
-    // closed form by the kernels.
+    // Free suffix: the last positions that all have the same back edges
+    // (none of them inside the suffix) and where each follows the one before
+    // it. Their completions are counted in closed form by the kernels.
     D.free_from = D.dend;
-    for (int p = D.dend - 1; p >= 1; --p) {
-        if (D.back[p] != 0)
-            break;
-        if (p < D.dend - 1 && !(D.sym[p + 1] >> p & 1u))
-            break;
-        D.free_from = p;
+    D.free_back = 0;
+    if (D.dend >= 2) {
+        const uint32_t B = D.back[D.dend - 1];
+        D.free_back = B;
+        for (int p = D.dend - 1; p >= 1; --p) {
+            if (D.back[p] != B || (B >> p & 1u))
+                break;
+            if (p < D.dend - 1 && !(D.sym[p + 1] >> p & 1u))
+                break;
+            D.free_from = p;
+        }
     }
     out->info = P;
     out->dev = D;

@@ -52,6 +52,21 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def profiled_traffic() -> dict:
+    """Per-launch DRAM bytes (read + write) of kernels captured with ncu, from
+    the summaries committed under profiles/ (lines
+    'traffic_bytes_per_launch[<kernel>]: <bytes>')."""
+    import glob
+    import re
+
+    out = {}
+    for path in glob.glob(os.path.join(ROOT, "profiles", "*.md")):
+        with open(path) as f:
+            for m in re.finditer(r"traffic_bytes_per_launch\[(\w+)\]:\s*([0-9.eE+]+)", f.read()):
+                out[m.group(1)] = float(m.group(2))
+    return out
+
+
 def gen_graph(kind, args):
     import beep_b200 as B
 
@@ -584,7 +599,10 @@ def main():
         "phases_ms_per_step": {"prep": prep_ms / args.steps, "count": count_ms / args.steps,
                                **{k: v[0] / args.steps for k, v in agg.items()}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "frac": achieved / peak if peak else None,
+                     "traffic": profiled_traffic().get({"small": "k_small", "medium": "k_medium",
+                                                        "large_dfs": "k_large_dfs",
+                                                        "large_rows": "k_large_rows"}[dom]),
                      "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                      else "fallback 6650 GB/s",
                      "bytes_per_launch": dom_bytes / max(dom_launches, 1),
