@@ -208,7 +208,8 @@ struct EnumCtx {
 
 __device__ __forceinline__ void emit_bits(const EnumCtx &ec, const uint32_t (&x)[kMaxQ], int P, uint64_t bits,
                                           uint32_t base) {
-    if (!bits)
+    // a pair that enumerates nothing may share an enumerating launch
+    if (!bits || ec.en.out == nullptr)
         return;
     if (*(volatile unsigned long long *)ec.en.n >= ec.en.k)
         return;
@@ -1114,8 +1115,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     lp->N = N;
     for (uint32_t i = 0; i < np; ++i) {
         hp[i].count = lp->d_counts + i;
-        if (hp[i].en.out)
-            hp[i].en.n = lp->d_counts + np + i;
+        hp[i].en.n = lp->d_counts + np + i; // every pair has a valid tuple counter (k = 0: none written)
     }
     BEEP_TRY(lp->alloc(lp->d_pairs, np));
     BEEP_TRY(lp->alloc(lp->d_offs, np + 1));

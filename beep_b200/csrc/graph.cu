@@ -356,9 +356,10 @@ beep_status keys_to_graph(Ctx *ctx, Graph *g, uint64_t *keys, uint64_t *keys_tmp
     BEEP_TRY(g->col.reserve((size_t)(m > 0 ? m : 1) * 4));
     uint32_t *deg = g->row_ptr.as<uint32_t>();
     BEEP_CUDA_TRY(cudaMemsetAsync(deg, 0, (size_t)(n + 1) * 4, s));
-    if (m > 0)
+    if (m > 0) {
         k_keys_to_coo<<<grid_for(m, 256, ctx->num_sms), 256, 0, s>>>(keys, m, g->col.as<uint32_t>(), deg);
         ++ctx->launches;
+    }
     BEEP_CUDA_TRY(cudaGetLastError());
     tb = 0;
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, deg, n + 1, s));
@@ -406,9 +407,10 @@ beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m
     BEEP_TRY(ctx->counter.reserve(64));
     unsigned *d_bad = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 32);
     BEEP_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 4, s));
-    if (n > 0)
+    if (n > 0) {
         k_check_csr<<<grid_for(n, 256, ctx->num_sms), 256, 0, s>>>(d_rp, d_col, n, m, d_bad);
         ++ctx->launches;
+    }
     BEEP_CUDA_TRY(cudaGetLastError());
     unsigned h_bad = 0;
     uint32_t h_m_end = 0;
@@ -434,9 +436,10 @@ beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m
     DevBuf keys, keys2;
     BEEP_TRY(keys.reserve((size_t)(m > 0 ? m : 1) * 8));
     BEEP_TRY(keys2.reserve((size_t)(m > 0 ? m : 1) * 8));
-    if (n > 0)
+    if (n > 0) {
         k_csr_keys<<<grid_for(n * 32, 256, ctx->num_sms), 256, 0, s>>>(d_rp, d_col, n, keys.as<uint64_t>());
         ++ctx->launches;
+    }
     BEEP_CUDA_TRY(cudaGetLastError());
     BEEP_TRY(keys_to_graph(ctx, g, keys.as<uint64_t>(), keys2.as<uint64_t>(), m, n));
     // validate ids
@@ -466,9 +469,10 @@ beep_status graph_build_from_device_edges(Ctx *ctx, Graph *g, int64_t ne, const 
     BEEP_TRY(ctx->counter.reserve(64));
     unsigned *d_max = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 48);
     BEEP_CUDA_TRY(cudaMemsetAsync(d_max, 0, 4, s));
-    if (ne > 0)
+    if (ne > 0) {
         k_edge_keys<<<grid_for(ne, 256, ctx->num_sms), 256, 0, s>>>(d_src, d_dst, ne, keys.as<uint64_t>(), d_max);
         ++ctx->launches;
+    }
     BEEP_CUDA_TRY(cudaGetLastError());
     unsigned h_max = 0;
     BEEP_CUDA_TRY(cudaMemcpyAsync(&h_max, d_max, 4, cudaMemcpyDeviceToHost, s));
@@ -503,9 +507,10 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     unsigned long long *d_removed = ctx->counter.as<unsigned long long>();
 
     const int gv = grid_for(n, 256, ctx->num_sms);
-    if (n > 0)
+    if (n > 0) {
         k_peel_init<<<gv, 256, 0, s>>>(rp, n, deg, alive);
         ++ctx->launches;
+    }
     BEEP_CUDA_TRY(cudaGetLastError());
     // Iterated peel: loop while a round removes more than 5% of n
     // (subgraph_matching.cuh:699-758).
@@ -520,9 +525,10 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
             BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, d_removed, 8, cudaMemcpyDeviceToHost, s));
             BEEP_CUDA_TRY(cudaStreamSynchronize(s));
             removed = ctx->h_pinned[0];
-            if (removed > 0)
+            if (removed > 0) {
                 k_peel_degree<<<gv, 256, 0, s>>>(rp, col, alive, n, deg);
                 ++ctx->launches;
+            }
             BEEP_CUDA_TRY(cudaGetLastError());
         }
         ++rounds;
@@ -538,9 +544,10 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
         ++hb;
     unsigned long long *d_alive = d_removed + 1;
     BEEP_CUDA_TRY(cudaMemsetAsync(d_alive, 0, 8, s));
-    if (n > 0)
+    if (n > 0) {
         k_prio_keys<<<gv, 256, 0, s>>>(deg, n, maxdeg, asc, keys, d_alive);
         ++ctx->launches;
+    }
     BEEP_CUDA_TRY(cudaGetLastError());
     size_t tb = 0;
     BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys, keys2, n, 0, 32 + hb, s));
