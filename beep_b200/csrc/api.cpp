@@ -1,7 +1,9 @@
 // api.cpp — the C ABI (include/beep.h) over the device graph build and the
 // counting kernels.
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 
 #include "internal.h"
 
@@ -29,13 +31,45 @@ beep_status bind(beep_ctx *ctx) {
 
 // Copy a host array to a device buffer through the context's stream.
 template <typename T> beep_status upload(Ctx *ctx, DevBuf &dst, const T *src, size_t count) {
-    BEEP_TRY(dst.reserve(std::max<size_t>(count, 1) * sizeof(T)));
+    BEEP_TRY(ctx->grow(dst, std::max<size_t>(count, 1) * sizeof(T)));
     if (count)
         BEEP_CUDA_TRY(cudaMemcpyAsync(dst.ptr, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
     return BEEP_OK;
 }
 
 } // namespace
+} // namespace beep
+
+namespace beep {
+namespace {
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+} // namespace
+
+bool trace_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("BEEP_TRACE");
+        return e && *e && *e != '0';
+    }();
+    return on;
+}
+
+PhaseTrace::PhaseTrace(const char *scope_, cudaStream_t s) : scope(scope_), stream(s), t0(0) {
+    if (trace_enabled()) {
+        cudaStreamSynchronize(stream);
+        t0 = now_ms();
+    }
+}
+
+void PhaseTrace::mark(const char *phase) {
+    if (!trace_enabled())
+        return;
+    cudaStreamSynchronize(stream);
+    const double t = now_ms();
+    std::fprintf(stderr, "beep-trace %s.%s %.3f ms\n", scope, phase, t - t0);
+    t0 = t;
+}
 } // namespace beep
 
 using namespace beep;
@@ -161,7 +195,9 @@ void graph_free(beep_graph *g) {
     cudaSetDevice(g->impl.device);
     if (ctx)
         cudaStreamSynchronize(ctx->impl.stream);
+    PhaseTrace tr("graph", ctx ? ctx->impl.stream : nullptr);
     delete g;
+    tr.mark("destroy");
     ctx_release(ctx);
 }
 } // namespace
@@ -491,8 +527,8 @@ beep_status beep_batch_destroy(beep_batch *b) {
         return BEEP_OK;
     beep_ctx *ctx = b->ctx;
     cudaSetDevice(ctx->impl.device);
-    b->plan.reset();
     cudaStreamSynchronize(ctx->impl.stream);
+    b->plan.reset();
     delete b;
     ctx_release(ctx);
     return BEEP_OK;

@@ -1052,6 +1052,7 @@ void LaunchPlanDeleter::operator()(LaunchPlan *p) const { delete p; }
 
 beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out) {
     cudaStream_t s = ctx->stream;
+    PhaseTrace tr("plan", s);
     LaunchPlanPtr lp(new LaunchPlan);
     lp->ctx = ctx;
     beep_stats &st = lp->st;
@@ -1101,6 +1102,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     }
     const uint32_t np = (uint32_t)hp.size();
     lp->np = np;
+    tr.mark("views");
     BEEP_TRY(ctx->host_results(np + 4, &lp->h_counts));
     BEEP_TRY(lp->alloc(lp->d_counts, 2 * (size_t)np + 4));
     lp->ncursors = 64;
@@ -1151,6 +1153,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     st.roots_medium = (int64_t)tier_n[1] + tier_n[2];
     st.roots_large = tier_n[3];
     st.roots = st.roots_small + st.roots_medium + st.roots_large;
+    tr.mark("classify");
     uint32_t next_cursor = 0;
     auto cursor = [&]() -> unsigned * { return lp->d_cursors + (next_cursor++ % lp->ncursors); };
 
@@ -1163,7 +1166,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         TierSel sel{lp->d_tier, (uint8_t)(k + 1)};
         unsigned *d_ns = d_misc + 80;
         BEEP_CUDA_TRY(cub::DeviceSelect::If(nullptr, tb, it, d_sel, d_ns, N, sel, s));
-        BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+        BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
         BEEP_CUDA_TRY(cub::DeviceSelect::If(ctx->scratch.ptr, tb, it, d_sel, d_ns, N, sel, s));
         const int by_domain = (k == 1 || k == 2) ? 1 : 0;
         int depths = 0;
@@ -1179,7 +1182,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             const int end_bit = by_domain ? 20 : 4;
             BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_keys, d_keys2, d_tmp_items, list, n_k, 0,
                                                           end_bit, s));
-            BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+            BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
             BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ctx->scratch.ptr, tb, d_keys, d_keys2, d_tmp_items, list,
                                                           n_k, 0, end_bit, s));
         }
@@ -1310,6 +1313,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             }
         }
     }
+    tr.mark("large_batches");
     // medium tiers: block per root, bitmap in shared memory
     for (int sub = 0; sub < 2; ++sub) {
         const int k = 1 + sub;
@@ -1378,6 +1382,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
 #undef BEEP_CASE
         }
     BEEP_CUDA_TRY(cudaStreamSynchronize(s)); // planning buffers are final
+    tr.mark("lists");
     *out = std::move(lp);
     return BEEP_OK;
 }
@@ -1628,7 +1633,11 @@ beep_status run_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t opt
         cudaEventDestroy(p1);
     }
     beep_stats st;
+    PhaseTrace tr("count", ctx->stream);
     BEEP_TRY(execute_plan(ctx, lp.get(), options, &specs, counts, specs.size(), &st));
+    tr.mark("execute");
+    lp.reset();
+    tr.mark("release");
     st.prep_ms = prep_ms;
     if (stats)
         *stats = st;

@@ -328,14 +328,14 @@ beep_status keys_to_graph(Ctx *ctx, Graph *g, uint64_t *keys, uint64_t *keys_tmp
     int end_bit = 64;
     size_t tb = 0;
     BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys, keys_tmp, nkeys, 0, end_bit, s));
-    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
     BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(ctx->scratch.ptr, tb, keys, keys_tmp, nkeys, 0, end_bit, s));
     // unique
-    BEEP_TRY(ctx->counter.reserve(64));
+    BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned long long *d_num = ctx->counter.as<unsigned long long>();
     tb = 0;
     BEEP_CUDA_TRY(cub::DeviceSelect::Unique(nullptr, tb, keys_tmp, keys, d_num, nkeys, s));
-    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
     BEEP_CUDA_TRY(cub::DeviceSelect::Unique(ctx->scratch.ptr, tb, keys_tmp, keys, d_num, nkeys, s));
     unsigned long long h_num = 0;
     BEEP_CUDA_TRY(cudaMemcpyAsync(&h_num, d_num, sizeof(h_num), cudaMemcpyDeviceToHost, s));
@@ -352,8 +352,8 @@ beep_status keys_to_graph(Ctx *ctx, Graph *g, uint64_t *keys, uint64_t *keys_tmp
         return fail(BEEP_ERR_UNSUPPORTED, "graph has 2^32 or more directed edges");
     g->n = n;
     g->m = m;
-    BEEP_TRY(g->row_ptr.reserve((size_t)(n + 1) * 4));
-    BEEP_TRY(g->col.reserve((size_t)(m > 0 ? m : 1) * 4));
+    BEEP_TRY(ctx->grow(g->row_ptr, (size_t)(n + 1) * 4));
+    BEEP_TRY(ctx->grow(g->col, (size_t)(m > 0 ? m : 1) * 4));
     uint32_t *deg = g->row_ptr.as<uint32_t>();
     BEEP_CUDA_TRY(cudaMemsetAsync(deg, 0, (size_t)(n + 1) * 4, s));
     if (m > 0) {
@@ -363,14 +363,14 @@ beep_status keys_to_graph(Ctx *ctx, Graph *g, uint64_t *keys, uint64_t *keys_tmp
     BEEP_CUDA_TRY(cudaGetLastError());
     tb = 0;
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, deg, n + 1, s));
-    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ctx->scratch.ptr, tb, deg, deg, n + 1, s));
     return BEEP_OK;
 }
 
 beep_status finish_graph(Ctx *ctx, Graph *g) {
     cudaStream_t s = ctx->stream;
-    BEEP_TRY(ctx->counter.reserve(64));
+    BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned long long *d = ctx->counter.as<unsigned long long>();
     BEEP_CUDA_TRY(cudaMemsetAsync(d, 0, 16, s));
     if (g->n > 0)
@@ -403,8 +403,9 @@ beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m
     cudaStream_t s = ctx->stream;
     if (n < 0 || m < 0 || n >= (int64_t)0xffffffffll || m >= (int64_t)0xffffffffll)
         return fail(BEEP_ERR_INVALID_ARG, "graph size out of range");
+    PhaseTrace tr("graph", s);
     // Fast path: rows already strictly increasing with no self loop.
-    BEEP_TRY(ctx->counter.reserve(64));
+    BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned *d_bad = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 32);
     BEEP_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 4, s));
     if (n > 0) {
@@ -421,16 +422,20 @@ beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m
         return fail(BEEP_ERR_INVALID_ARG, "row_ptr[n] != m");
     if (h_bad & 2u)
         return fail(BEEP_ERR_INVALID_ARG, "row_ptr is not non-decreasing within [0, m]");
+    tr.mark("check");
     if (!h_bad) {
         g->n = n;
         g->m = m;
-        BEEP_TRY(g->row_ptr.reserve((size_t)(n + 1) * 4));
-        BEEP_TRY(g->col.reserve((size_t)(m > 0 ? m : 1) * 4));
+        BEEP_TRY(ctx->grow(g->row_ptr, (size_t)(n + 1) * 4));
+        BEEP_TRY(ctx->grow(g->col, (size_t)(m > 0 ? m : 1) * 4));
         if (g->row_ptr.ptr != (const void *)d_rp)
             BEEP_CUDA_TRY(cudaMemcpyAsync(g->row_ptr.ptr, d_rp, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, s));
         if (m > 0 && g->col.ptr != (const void *)d_col)
             BEEP_CUDA_TRY(cudaMemcpyAsync(g->col.ptr, d_col, (size_t)m * 4, cudaMemcpyDeviceToDevice, s));
-        return finish_graph(ctx, g);
+        tr.mark("copy");
+        beep_status st = finish_graph(ctx, g);
+        tr.mark("stats");
+        return st;
     }
     // Slow path: sort + unique packed (src, dst) keys. Out-of-range ids fail.
     DevBuf keys, keys2;
@@ -448,7 +453,7 @@ beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m
         size_t tb = 0;
         unsigned *d_max = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 40);
         BEEP_CUDA_TRY(cub::DeviceReduce::Max(nullptr, tb, g->col.as<uint32_t>(), d_max, g->m, s));
-        BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+        BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
         BEEP_CUDA_TRY(cub::DeviceReduce::Max(ctx->scratch.ptr, tb, g->col.as<uint32_t>(), d_max, g->m, s));
         BEEP_CUDA_TRY(cudaMemcpyAsync(&maxc, d_max, 4, cudaMemcpyDeviceToHost, s));
         BEEP_CUDA_TRY(cudaStreamSynchronize(s));
@@ -466,7 +471,7 @@ beep_status graph_build_from_device_edges(Ctx *ctx, Graph *g, int64_t ne, const 
     DevBuf keys, keys2;
     BEEP_TRY(keys.reserve((size_t)(ne > 0 ? ne : 1) * 8));
     BEEP_TRY(keys2.reserve((size_t)(ne > 0 ? ne : 1) * 8));
-    BEEP_TRY(ctx->counter.reserve(64));
+    BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned *d_max = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 48);
     BEEP_CUDA_TRY(cudaMemsetAsync(d_max, 0, 4, s));
     if (ne > 0) {
@@ -494,7 +499,7 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     const int64_t nn = n > 0 ? n : 1;
     size_t need = Carve::need({(size_t)nn * 4, (size_t)nn, (size_t)nn * 4, (size_t)nn * 8, (size_t)nn * 8,
                                (size_t)nn * 4, (size_t)(m > 0 ? m : 1) * 4});
-    BEEP_TRY(ctx->scratch2.reserve(need));
+    BEEP_TRY(ctx->grow(ctx->scratch2, need));
     Carve cv(ctx->scratch2.ptr);
     uint32_t *deg = cv.take<uint32_t>(nn);
     uint8_t *alive = cv.take<uint8_t>(nn);
@@ -503,9 +508,10 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     uint64_t *keys2 = cv.take<uint64_t>(nn);
     uint32_t *new_deg = cv.take<uint32_t>(nn);
     uint32_t *col_tmp = cv.take<uint32_t>(m > 0 ? m : 1);
-    BEEP_TRY(ctx->counter.reserve(64));
+    BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned long long *d_removed = ctx->counter.as<unsigned long long>();
 
+    PhaseTrace tr("view", s);
     const int gv = grid_for(n, 256, ctx->num_sms);
     if (n > 0) {
         k_peel_init<<<gv, 256, 0, s>>>(rp, n, deg, alive);
@@ -536,6 +542,7 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
             break;
     }
     v->peel_rounds = rounds;
+    tr.mark("peel");
 
     // Relabel by priority.
     const uint32_t maxdeg = (uint32_t)g->max_degree;
@@ -551,61 +558,58 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_CUDA_TRY(cudaGetLastError());
     size_t tb = 0;
     BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys, keys2, n, 0, 32 + hb, s));
-    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
     BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(ctx->scratch.ptr, tb, keys, keys2, n, 0, 32 + hb, s));
     // number of vertices that kept an edge
     BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, d_alive, 8, cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     const int64_t na = (int64_t)ctx->h_pinned[0];
     v->n = na;
-    BEEP_TRY(v->row_ptr.reserve((size_t)(na + 1) * 4));
-    BEEP_TRY(v->orig.reserve((size_t)(na > 0 ? na : 1) * 4));
-    BEEP_TRY(v->split.reserve((size_t)(na > 0 ? na : 1) * 4));
+    tr.mark("order");
+    BEEP_TRY(ctx->grow(v->row_ptr, (size_t)(na + 1) * 4));
+    BEEP_TRY(ctx->grow(v->orig, (size_t)(na > 0 ? na : 1) * 4));
+    BEEP_TRY(ctx->grow(v->split, (size_t)(na > 0 ? na : 1) * 4));
     BEEP_CUDA_TRY(cudaMemsetAsync(rank, 0xff, (size_t)nn * 4, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(new_deg, 0, (size_t)nn * 4, s));
-    if (na > 0)
+    if (na > 0) {
         k_rank<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(keys2, na, v->orig.as<uint32_t>(), rank, deg,
                                                                new_deg);
+        ++ctx->launches;
+    }
     BEEP_CUDA_TRY(cudaGetLastError());
     uint32_t *nrp = v->row_ptr.as<uint32_t>();
     tb = 0;
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, new_deg, nrp, na + 1, s));
-    BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+    BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ctx->scratch.ptr, tb, new_deg, nrp, na + 1, s));
     uint32_t h_m = 0;
     BEEP_CUDA_TRY(cudaMemcpyAsync(&h_m, nrp + na, 4, cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     v->m = h_m;
-    BEEP_TRY(v->col.reserve((size_t)(h_m > 0 ? h_m : 1) * 4));
-    if (na > 0)
+    tr.mark("rank_scan");
+    BEEP_TRY(ctx->grow(v->col, (size_t)(h_m > 0 ? h_m : 1) * 4));
+    if (na > 0) {
         k_fill_rows<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(rp, col, v->orig.as<uint32_t>(), rank,
                                                                            nrp, na, col_tmp);
+        ++ctx->launches;
+    }
     BEEP_CUDA_TRY(cudaGetLastError());
+    tr.mark("fill");
     if (h_m > 0) {
         tb = 0;
         BEEP_CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(nullptr, tb, col_tmp, v->col.as<uint32_t>(), (int64_t)h_m,
                                                          na, nrp, nrp + 1, s));
-        BEEP_TRY(ctx->scratch.reserve(tb + 1024));
+        BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
         BEEP_CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(ctx->scratch.ptr, tb, col_tmp, v->col.as<uint32_t>(),
                                                          (int64_t)h_m, na, nrp, nrp + 1, s));
     }
-    if (na > 0)
+    if (na > 0) {
         k_split<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(nrp, v->col.as<uint32_t>(), na,
                                                                 v->split.as<uint32_t>());
-    BEEP_CUDA_TRY(cudaGetLastError());
-    // max degree of the view
-    {
-        uint32_t *d_mx = reinterpret_cast<uint32_t *>(d_removed + 2);
-        BEEP_CUDA_TRY(cudaMemsetAsync(d_mx, 0, 4, s));
-        tb = 0;
-        BEEP_CUDA_TRY(cub::DeviceReduce::Max(nullptr, tb, new_deg, d_mx, na > 0 ? na : 1, s));
-        BEEP_TRY(ctx->scratch.reserve(tb + 1024));
-        BEEP_CUDA_TRY(cub::DeviceReduce::Max(ctx->scratch.ptr, tb, new_deg, d_mx, na > 0 ? na : 1, s));
-        uint32_t mx = 0;
-        BEEP_CUDA_TRY(cudaMemcpyAsync(&mx, d_mx, 4, cudaMemcpyDeviceToHost, s));
-        BEEP_CUDA_TRY(cudaStreamSynchronize(s));
-        v->max_deg = (int32_t)mx;
+        ++ctx->launches;
     }
+    BEEP_CUDA_TRY(cudaGetLastError());
+    tr.mark("sort_split");
     return BEEP_OK;
 }
 

@@ -17,6 +17,19 @@
 namespace beep {
 
 // ---------------------------------------------------------------------------
+// host phase trace: with BEEP_TRACE=1 in the environment, each marked phase
+// synchronises its stream and prints its wall-clock time to stderr
+// ---------------------------------------------------------------------------
+bool trace_enabled();
+struct PhaseTrace {
+    const char *scope;
+    cudaStream_t stream;
+    double t0;
+    PhaseTrace(const char *scope_, cudaStream_t s);
+    void mark(const char *phase);
+};
+
+// ---------------------------------------------------------------------------
 // errors
 // ---------------------------------------------------------------------------
 void set_error(const std::string &msg);
@@ -74,15 +87,24 @@ beep_status compile_plan(int32_t qn, const std::vector<int32_t> &qrow_ptr, const
 struct DevBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
+    bool pooled = false; // from a context's stream-ordered pool
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
+    // Owners release a buffer only after the work that uses it has completed
+    // (they synchronise its stream first), so a pooled buffer goes back to
+    // its pool at once.
     void release() {
-        if (ptr)
-            cudaFree(ptr);
+        if (ptr) {
+            if (pooled)
+                cudaFreeAsync(ptr, cudaStreamPerThread);
+            else
+                cudaFree(ptr);
+        }
         ptr = nullptr;
         bytes = 0;
+        pooled = false;
     }
     // Grow-only: keeps the allocation when it is already large enough.
     beep_status reserve(size_t b) {
@@ -100,6 +122,36 @@ struct DevBuf {
         bytes = b;
         return BEEP_OK;
     }
+    // Grow-only, from a stream-ordered pool: the old buffer is freed in the
+    // order of stream s (work already queued on s may still read it) and the
+    // new one is usable on s at once. Pool allocations cost microseconds where
+    // cudaMalloc/cudaFree cost up to milliseconds and synchronise the device.
+    beep_status reserve(size_t b, cudaMemPool_t pool, cudaStream_t s) {
+        if (b <= bytes && ptr)
+            return BEEP_OK;
+        if (!pool)
+            return reserve(b);
+        if (ptr) {
+            if (pooled)
+                cudaFreeAsync(ptr, s);
+            else
+                cudaFree(ptr);
+        }
+        ptr = nullptr;
+        bytes = 0;
+        pooled = false;
+        if (b == 0)
+            b = 16;
+        cudaError_t e = cudaMallocFromPoolAsync(&ptr, b, pool, s);
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            return fail(BEEP_ERR_OUT_OF_MEMORY, std::string("device pool allocation of ") + std::to_string(b) +
+                                                    " bytes: " + cudaGetErrorString(e));
+        }
+        bytes = b;
+        pooled = true;
+        return BEEP_OK;
+    }
     template <typename T> T *as() const { return static_cast<T *>(ptr); }
 };
 
@@ -111,7 +163,6 @@ struct View {
     int32_t asc = 1;
     int64_t n = 0;           // vertices with degree > 0 after peeling
     int64_t m = 0;           // directed edges
-    int32_t max_deg = 0;
     int32_t peel_rounds = 0;
     DevBuf row_ptr;          // u32[n+1]
     DevBuf col;              // u32[m], new ids, rows ascending
@@ -148,6 +199,8 @@ struct Ctx {
     unsigned long long *h_pinned = nullptr; // pinned host mirror of small results
     uint64_t launches = 0; // kernels of this library launched on the context
     cudaMemPool_t pool = nullptr; // stream-ordered pool for per-call buffers
+    // grow b (a buffer of this context or of an object it builds) from the pool on the context's stream
+    beep_status grow(DevBuf &b, size_t bytes) { return b.reserve(bytes, pool, stream); }
     // side streams and events that let the kernel tiers of one call overlap
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};

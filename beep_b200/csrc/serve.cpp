@@ -299,17 +299,10 @@ beep_status beep_serve_create(beep_ctx *ctx, const beep_serve_options *opt, beep
         S.count_options = opt->count_options & BEEP_OPT_REFERENCE_ROOT_CAP;
     }
     cudaError_t e = cudaMallocHost(&S.ctx.h_pinned, 64);
-    cudaMemPoolProps props;
-    std::memset(&props, 0, sizeof(props));
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = S.ctx.device;
-    if (e == cudaSuccess)
-        e = cudaMemPoolCreate(&S.ctx.pool, &props);
-    if (e == cudaSuccess) {
-        uint64_t keep = ~0ull;
-        e = cudaMemPoolSetAttribute(S.ctx.pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
+    // buffers come from the user context's pool (the server holds a
+    // reference to that context, so the pool outlives everything built here,
+    // including the views it caches in the graphs)
+    S.ctx.pool = ctx->impl.pool;
     S.slots.resize(nstreams);
     for (auto &sl : S.slots) {
         if (e == cudaSuccess)
@@ -485,8 +478,7 @@ beep_status beep_serve_destroy(beep_server *s) {
         if (sl.ev_fork)
             cudaEventDestroy(sl.ev_fork);
     }
-    if (S.ctx.pool)
-        cudaMemPoolDestroy(S.ctx.pool);
+    S.ctx.pool = nullptr; // borrowed
     for (auto &sl : S.slots)
         if (sl.stream)
             cudaStreamDestroy(sl.stream);
