@@ -21,10 +21,52 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// Rows are processed in two passes so that a few very long rows (hubs, which
+// the priority order and R-MAT-like inputs put next to each other) cannot
+// serialise on one warp: rows of up to kSerialMax entries are handled by one
+// lane each; longer rows are cut into chunks of kChunk entries that the first
+// pass appends to a list, and a second kernel spreads the chunks over every
+// warp of the GPU.
+constexpr uint32_t kSerialMax = 32;
+constexpr uint32_t kChunk = 1024;
+
+struct RowChunk {
+    uint32_t row, b, e, pad;
+};
+
+// Warp-collective: lane l appends the chunks of [b, e) of row `row` when
+// `big` (one atomic per warp).
+// Entries past `cap` are dropped (only an invalid CSR, whose rows overlap, can
+// have more chunks than a valid one); readers clamp the count to `cap`.
+__device__ __forceinline__ void push_chunks(bool big, uint32_t row, uint32_t b, uint32_t e, RowChunk *list,
+                                            unsigned *n_list, uint32_t cap, int lane) {
+    const uint32_t nc = big ? (uint32_t)(((uint64_t)e - b + kChunk - 1) / kChunk) : 0u;
+    uint32_t inc = nc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o)
+            inc += t;
+    }
+    const uint32_t total = __shfl_sync(kFull, inc, 31);
+    if (total == 0)
+        return;
+    uint32_t base = 0;
+    if (lane == 31)
+        base = atomicAdd(n_list, total);
+    base = __shfl_sync(kFull, base, 31);
+    const uint32_t pos = base + inc - nc;
+    for (uint32_t c = 0; c < nc && pos + c < cap; ++c) {
+        const uint32_t cb = b + c * kChunk;
+        list[pos + c] = RowChunk{row, cb, min(cb + kChunk, e), 0u};
+    }
+}
+
+// Capacity of a chunk list for a CSR of n rows and m entries.
+inline size_t chunk_capacity(int64_t n, int64_t m) { return (size_t)n + (size_t)m / kChunk + 64; }
+
 __global__ void k_check_csr(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n, int64_t m,
-                            unsigned *bad) {
-    // Lane l checks vertex base + l alone when its row has <= 32 entries;
-    // longer rows are checked by the whole warp afterwards.
+                            unsigned *bad, RowChunk *chunks, unsigned *n_chunks, uint32_t cap) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     unsigned flag = 0;
@@ -37,7 +79,7 @@ __global__ void k_check_csr(const uint32_t *__restrict__ rp, const uint32_t *__r
             e = rp[v + 1];
             if (e < b || e > m)
                 flag |= 2u; // row pointers unusable
-            else if (e - b > 32)
+            else if (e - b > kSerialMax)
                 big = true;
             else
                 for (uint32_t i = b; i < e; ++i) {
@@ -46,17 +88,27 @@ __global__ void k_check_csr(const uint32_t *__restrict__ rp, const uint32_t *__r
                         flag |= 1u;
                 }
         }
-        unsigned mask = __ballot_sync(kFull, big);
-        while (mask) {
-            const int L = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const uint32_t u = (uint32_t)(base + L);
-            const uint32_t ub = __shfl_sync(kFull, b, L), ue = __shfl_sync(kFull, e, L);
-            for (uint32_t i = ub + lane; i < ue; i += 32) {
-                const uint32_t w = col[i];
-                if (!(w < n && w != u && (i == ub || col[i - 1] < w)))
-                    flag |= 1u;
-            }
+        push_chunks(big, (uint32_t)v, b, e, chunks, n_chunks, cap, lane);
+    }
+    flag = __reduce_or_sync(kFull, flag);
+    if (lane == 0 && flag)
+        atomicOr(bad, flag);
+}
+
+__global__ void k_check_chunks(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n,
+                               const RowChunk *__restrict__ chunks, const unsigned *__restrict__ n_chunks,
+                               uint32_t cap, unsigned *bad) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t nc = min(*n_chunks, cap);
+    unsigned flag = 0;
+    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc; c += warps) {
+        const RowChunk ch = chunks[c];
+        const uint32_t rb = rp[ch.row];
+        for (uint32_t i = ch.b + lane; i < ch.e; i += 32) {
+            const uint32_t w = col[i];
+            if (!(w < n && w != ch.row && (i == rb || col[i - 1] < w)))
+                flag |= 1u;
         }
     }
     flag = __reduce_or_sync(kFull, flag);
@@ -150,8 +202,8 @@ __global__ void k_peel_mark(const uint32_t *__restrict__ deg, uint8_t *alive, in
 // (remove_edges_connected_to_node + warp_detect_deleted_edges,
 // common_utils.cuh:99-133, 217-246).
 __global__ void k_peel_degree(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
-                              const uint8_t *__restrict__ alive, int64_t n, uint32_t *deg) {
-    // lane-serial for rows of <= 32 entries, warp-cooperative for longer ones
+                              const uint8_t *__restrict__ alive, int64_t n, uint32_t *deg, RowChunk *chunks,
+                              unsigned *n_chunks, uint32_t cap) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += warps * 32) {
@@ -164,8 +216,9 @@ __global__ void k_peel_degree(const uint32_t *__restrict__ rp, const uint32_t *_
             } else {
                 b = rp[v];
                 e = rp[v + 1];
-                if (e - b > 32) {
+                if (e - b > kSerialMax) {
                     big = true;
+                    deg[v] = 0; // the chunks add their counts
                 } else {
                     uint32_t c = 0;
                     for (uint32_t i = b; i < e; ++i)
@@ -174,18 +227,24 @@ __global__ void k_peel_degree(const uint32_t *__restrict__ rp, const uint32_t *_
                 }
             }
         }
-        unsigned mask = __ballot_sync(kFull, big);
-        while (mask) {
-            const int L = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const uint32_t ub = __shfl_sync(kFull, b, L), ue = __shfl_sync(kFull, e, L);
-            uint32_t c = 0;
-            for (uint32_t i = ub + lane; i < ue; i += 32)
-                c += alive[col[i]];
-            c = __reduce_add_sync(kFull, c);
-            if (lane == 0)
-                deg[base + L] = c;
-        }
+        push_chunks(big, (uint32_t)v, b, e, chunks, n_chunks, cap, lane);
+    }
+}
+
+__global__ void k_peel_chunks(const uint32_t *__restrict__ col, const uint8_t *__restrict__ alive,
+                              const RowChunk *__restrict__ chunks, const unsigned *__restrict__ n_chunks,
+                              uint32_t cap, uint32_t *deg) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t nc = min(*n_chunks, cap);
+    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc; c += warps) {
+        const RowChunk ch = chunks[c];
+        uint32_t k = 0;
+        for (uint32_t i = ch.b + lane; i < ch.e; i += 32)
+            k += alive[col[i]];
+        k = __reduce_add_sync(kFull, k);
+        if (lane == 0 && k)
+            atomicAdd(&deg[ch.row], k);
     }
 }
 
@@ -226,27 +285,29 @@ __global__ void k_rank(const uint64_t *__restrict__ keys, int64_t n_alive, uint3
 }
 
 // Row i of the relabelled graph: ranks of the surviving neighbours of
-// orig[i], compacted in input order (sorted afterwards).
+// orig[i], in any order (the rows are sorted afterwards). Short rows keep
+// input order; the chunks of long rows take their places in the row through
+// a per-row cursor (cursor[i], zeroed here).
 __global__ void k_fill_rows(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
                             const uint32_t *__restrict__ orig, const uint32_t *__restrict__ rank,
-                            const uint32_t *__restrict__ new_rp, int64_t n_alive, uint32_t *new_col) {
-    // lane-serial for rows of <= 32 entries, warp-cooperative (ballot
-    // compaction) for longer ones
+                            const uint32_t *__restrict__ new_rp, int64_t n_alive, uint32_t *new_col,
+                            uint32_t *cursor, RowChunk *chunks, unsigned *n_chunks, uint32_t cap) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n_alive;
          base += warps * 32) {
         const int64_t i = base + lane;
         bool big = false;
-        uint32_t b = 0, e = 0, out = 0;
+        uint32_t b = 0, e = 0;
         if (i < n_alive) {
             const uint32_t v = orig[i];
             b = rp[v];
             e = rp[v + 1];
-            out = new_rp[i];
-            if (e - b > 32) {
+            if (e - b > kSerialMax) {
                 big = true;
+                cursor[i] = 0;
             } else {
+                uint32_t out = new_rp[i];
                 for (uint32_t k = b; k < e; ++k) {
                     const uint32_t r = rank[col[k]];
                     if (r != 0xffffffffu)
@@ -254,23 +315,35 @@ __global__ void k_fill_rows(const uint32_t *__restrict__ rp, const uint32_t *__r
                 }
             }
         }
-        unsigned mask = __ballot_sync(kFull, big);
-        while (mask) {
-            const int L = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const uint32_t ub = __shfl_sync(kFull, b, L), ue = __shfl_sync(kFull, e, L);
-            uint32_t o = __shfl_sync(kFull, out, L);
-            for (uint32_t k0 = ub; k0 < ue; k0 += 32) {
-                const uint32_t k = k0 + lane;
-                uint32_t r = 0xffffffffu;
-                if (k < ue)
-                    r = rank[col[k]];
-                const bool keep = r != 0xffffffffu;
-                const unsigned bal = __ballot_sync(kFull, keep);
-                if (keep)
-                    new_col[o + __popc(bal & ((1u << lane) - 1u))] = r;
-                o += __popc(bal);
-            }
+        push_chunks(big, (uint32_t)i, b, e, chunks, n_chunks, cap, lane);
+    }
+}
+
+__global__ void k_fill_chunks(const uint32_t *__restrict__ col, const uint32_t *__restrict__ rank,
+                              const uint32_t *__restrict__ new_rp, const RowChunk *__restrict__ chunks,
+                              const unsigned *__restrict__ n_chunks, uint32_t cap, uint32_t *cursor,
+                              uint32_t *new_col) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t nc = min(*n_chunks, cap);
+    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc; c += warps) {
+        const RowChunk ch = chunks[c];
+        const uint32_t row_base = new_rp[ch.row];
+        for (uint32_t k0 = ch.b; k0 < ch.e; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            uint32_t r = 0xffffffffu;
+            if (k < ch.e)
+                r = rank[col[k]];
+            const bool keep = r != 0xffffffffu;
+            const unsigned bal = __ballot_sync(kFull, keep);
+            if (!bal)
+                continue;
+            uint32_t at = 0;
+            if (lane == 0)
+                at = atomicAdd(&cursor[ch.row], (uint32_t)__popc(bal));
+            at = __shfl_sync(kFull, at, 0);
+            if (keep)
+                new_col[row_base + at + __popc(bal & ((1u << lane) - 1u))] = r;
         }
     }
 }
@@ -407,10 +480,16 @@ beep_status graph_build_from_device_csr(Ctx *ctx, Graph *g, int64_t n, int64_t m
     // Fast path: rows already strictly increasing with no self loop.
     BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned *d_bad = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 32);
-    BEEP_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 4, s));
+    unsigned *d_nchunks = reinterpret_cast<unsigned *>(ctx->counter.as<char>() + 36);
+    BEEP_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 8, s));
     if (n > 0) {
-        k_check_csr<<<grid_for(n, 256, ctx->num_sms), 256, 0, s>>>(d_rp, d_col, n, m, d_bad);
-        ++ctx->launches;
+        BEEP_TRY(ctx->grow(ctx->scratch2, chunk_capacity(n, m) * sizeof(RowChunk)));
+        RowChunk *chunks = ctx->scratch2.as<RowChunk>();
+        const uint32_t cap = (uint32_t)std::min<size_t>(chunk_capacity(n, m), 0xffffffffu);
+        k_check_csr<<<grid_for(n, 256, ctx->num_sms), 256, 0, s>>>(d_rp, d_col, n, m, d_bad, chunks, d_nchunks,
+                                                                     cap);
+        k_check_chunks<<<ctx->num_sms * 8, 256, 0, s>>>(d_rp, d_col, n, chunks, d_nchunks, cap, d_bad);
+        ctx->launches += 2;
     }
     BEEP_CUDA_TRY(cudaGetLastError());
     unsigned h_bad = 0;
@@ -497,8 +576,9 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     const uint32_t *rp = g->row_ptr.as<uint32_t>();
     const uint32_t *col = g->col.as<uint32_t>();
     const int64_t nn = n > 0 ? n : 1;
+    const size_t cap = chunk_capacity(n, m);
     size_t need = Carve::need({(size_t)nn * 4, (size_t)nn, (size_t)nn * 4, (size_t)nn * 8, (size_t)nn * 8,
-                               (size_t)nn * 4, (size_t)(m > 0 ? m : 1) * 4});
+                               (size_t)nn * 4, (size_t)(m > 0 ? m : 1) * 4, cap * sizeof(RowChunk), 16});
     BEEP_TRY(ctx->grow(ctx->scratch2, need));
     Carve cv(ctx->scratch2.ptr);
     uint32_t *deg = cv.take<uint32_t>(nn);
@@ -508,6 +588,9 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     uint64_t *keys2 = cv.take<uint64_t>(nn);
     uint32_t *new_deg = cv.take<uint32_t>(nn);
     uint32_t *col_tmp = cv.take<uint32_t>(m > 0 ? m : 1);
+    RowChunk *chunks = cv.take<RowChunk>(cap);
+    unsigned *d_nchunks = cv.take<unsigned>(4);
+    const uint32_t ucap = (uint32_t)std::min<size_t>(cap, 0xffffffffu);
     BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned long long *d_removed = ctx->counter.as<unsigned long long>();
 
@@ -532,8 +615,10 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
             BEEP_CUDA_TRY(cudaStreamSynchronize(s));
             removed = ctx->h_pinned[0];
             if (removed > 0) {
-                k_peel_degree<<<gv, 256, 0, s>>>(rp, col, alive, n, deg);
-                ++ctx->launches;
+                BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks, 0, 4, s));
+                k_peel_degree<<<gv, 256, 0, s>>>(rp, col, alive, n, deg, chunks, d_nchunks, ucap);
+                k_peel_chunks<<<ctx->num_sms * 8, 256, 0, s>>>(col, alive, chunks, d_nchunks, ucap, deg);
+                ctx->launches += 2;
             }
             BEEP_CUDA_TRY(cudaGetLastError());
         }
@@ -589,9 +674,12 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     tr.mark("rank_scan");
     BEEP_TRY(ctx->grow(v->col, (size_t)(h_m > 0 ? h_m : 1) * 4));
     if (na > 0) {
+        BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks, 0, 4, s));
         k_fill_rows<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(rp, col, v->orig.as<uint32_t>(), rank,
-                                                                           nrp, na, col_tmp);
-        ++ctx->launches;
+                                                                           nrp, na, col_tmp, new_deg, chunks,
+                                                                           d_nchunks, ucap);
+        k_fill_chunks<<<ctx->num_sms * 8, 256, 0, s>>>(col, rank, nrp, chunks, d_nchunks, ucap, new_deg, col_tmp);
+        ctx->launches += 2;
     }
     BEEP_CUDA_TRY(cudaGetLastError());
     tr.mark("fill");
