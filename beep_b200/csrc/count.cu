@@ -382,56 +382,76 @@ __device__ __forceinline__ uint32_t upper_bound_g(const uint32_t *__restrict__ a
     return lo;
 }
 
-// Exclusive prefix of buf[0, R) in place, total in buf[R]; one warp.
-__device__ __forceinline__ void warp_excl_scan(uint32_t *buf, uint32_t R, int lane) {
+// Exclusive prefix of buf[0, R) in place, total in buf[R], by a group of G
+// lanes (G = 32: a warp) whose mask is gmask; glane is the lane within it.
+template <int G>
+__device__ __forceinline__ void group_excl_scan(uint32_t *buf, uint32_t R, int glane, unsigned gmask) {
     uint32_t carry = 0;
-    for (uint32_t base = 0; base < R; base += 32) {
-        const uint32_t idx = base + lane;
+    for (uint32_t base = 0; base < R; base += G) {
+        const uint32_t idx = base + glane;
         const uint32_t x = idx < R ? buf[idx] : 0u;
         uint32_t inc = x;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(kFull, inc, o);
-            if (lane >= o)
+        for (int o = 1; o < G; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(gmask, inc, o, G);
+            if (glane >= o)
                 inc += y;
         }
         if (idx < R)
             buf[idx] = carry + inc - x;
-        carry += __shfl_sync(kFull, inc, 31);
+        carry += __shfl_sync(gmask, inc, G - 1, G);
     }
-    if (lane == 0)
+    if (glane == 0)
         buf[R] = carry;
 }
 
-template <bool BLOCK> __device__ __forceinline__ void group_sync() {
-    if constexpr (BLOCK)
-        __syncthreads();
-    else
-        __syncwarp();
+__device__ __forceinline__ void warp_excl_scan(uint32_t *buf, uint32_t R, int lane) {
+    group_excl_scan<32>(buf, R, lane, kFull);
 }
 
-template <bool BLOCK, typename SetFn>
+// G = 0: the whole block; else a group of G lanes of one warp.
+template <int G> __device__ __forceinline__ void group_sync(unsigned gmask) {
+    if constexpr (G == 0)
+        __syncthreads();
+    else
+        __syncwarp(gmask);
+}
+
+// Lists longer than this are first cut to [min, max] of the A entries they
+// can meet (two binary searches); shorter ones are searched whole, which
+// costs fewer dependent loads.
+constexpr uint32_t kTrimMin = 16;
+
+template <int G, typename SetFn>
 __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const uint32_t *A, uint32_t D,
                                                 uint32_t i0, uint32_t i1, uint32_t *s_hb, uint32_t *s_pre,
-                                                uint32_t tid, uint32_t nthr, SetFn set) {
+                                                uint32_t tid, uint32_t nthr, unsigned gmask, SetFn set) {
     const uint32_t R = i1 - i0;
     for (uint32_t r = tid; r < R; r += nthr) {
         const uint32_t i = i0 + r;
         uint32_t hb, he, xb, xe, c = 0;
         hd_range(v, asc, A[i], i, D, hb, he, xb, xe);
         if (xb < xe && hb < he) {
-            const uint32_t lo = lower_bound_g(v.col, hb, he, A[xb]);
-            const uint32_t hi = upper_bound_g(v.col, lo, he, A[xe - 1]);
-            hb = lo;
-            c = hi - lo;
+            if (he - hb > kTrimMin) {
+                const uint32_t lo = lower_bound_g(v.col, hb, he, A[xb]);
+                const uint32_t hi = upper_bound_g(v.col, lo, he, A[xe - 1]);
+                hb = lo;
+                c = hi - lo;
+            } else {
+                c = he - hb;
+            }
         }
         s_hb[r] = hb;
         s_pre[r] = c;
     }
-    group_sync<BLOCK>();
-    if (tid < 32)
-        warp_excl_scan(s_pre, R, (int)tid);
-    group_sync<BLOCK>();
+    group_sync<G>(gmask);
+    if constexpr (G == 0) {
+        if (tid < 32)
+            warp_excl_scan(s_pre, R, (int)tid);
+    } else {
+        group_excl_scan<G>(s_pre, R, (int)tid, gmask);
+    }
+    group_sync<G>(gmask);
     const uint32_t T = s_pre[R];
     for (uint32_t t = tid; t < T; t += nthr) {
         // row r: last with s_pre[r] <= t
@@ -507,30 +527,43 @@ __device__ __forceinline__ void pair_domain(const PairRegs &pr, uint32_t r, uint
 }
 
 // ---------------------------------------------------------------------------
-// small tier: warp per root, 64-bit rows, one lane per level-1 vertex
+// small tier: a group of G lanes per root (G = 8 for domains of at most
+// kTinyMaxD vertices, four roots per warp; G = 32 up to kSmallMaxD), 64-bit
+// rows, one lane per level-1 vertex
 // ---------------------------------------------------------------------------
 constexpr int kSmallWarps = 8;
+constexpr int kTinyMaxD = 16;
 
-template <int DEND, bool ENUM>
+template <int G> __device__ __forceinline__ unsigned long long group_sum(unsigned long long v, unsigned gmask) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1)
+        v += __shfl_xor_sync(gmask, v, o, G);
+    return v;
+}
+
+template <int DEND, bool ENUM, int G, int MAXD>
 __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__restrict__ pairs,
                                                            const uint64_t *__restrict__ items, uint32_t nitems) {
-    __shared__ uint64_t s_rows[kSmallWarps][kSmallMaxD];
-    __shared__ uint32_t s_A[kSmallWarps][kSmallMaxD];
-    __shared__ uint32_t s_hb[kSmallWarps][kSmallMaxD];
-    __shared__ uint32_t s_pre[kSmallWarps][kSmallMaxD + 1];
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint64_t *rows = s_rows[wib];
-    uint32_t *A = s_A[wib];
+    constexpr int NG = kSmallWarps * 32 / G; // groups per block
+    __shared__ uint64_t s_rows[NG][MAXD];
+    __shared__ uint32_t s_A[NG][MAXD];
+    __shared__ uint32_t s_hb[NG][MAXD];
+    __shared__ uint32_t s_pre[NG][MAXD + 1];
+    const int gid = threadIdx.x / G, glane = threadIdx.x % G;
+    const int lane = threadIdx.x & 31;
+    const unsigned gmask = G == 32 ? kFull : (((1u << G) - 1u) << (lane & ~(G - 1)));
+    uint64_t *rows = s_rows[gid];
+    uint32_t *A = s_A[gid];
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
     EnumCtx ec;
     unsigned long long cnt = 0;
-    for (uint32_t ri = blockIdx.x * kSmallWarps + wib; ri < nitems; ri += gridDim.x * kSmallWarps) {
+    for (uint32_t ri = blockIdx.x * NG + gid; ri < nitems; ri += gridDim.x * NG) {
         const uint64_t it = items[ri];
         const uint32_t p = item_pair(it), r = item_root(it);
-        if (p != cur) { // warp-uniform
-            cnt = warp_sum(cnt);
-            if (lane == 0 && cnt)
+        if (p != cur) { // group-uniform
+            cnt = group_sum<G>(cnt, gmask);
+            if (glane == 0 && cnt)
                 atomicAdd(pr.count, cnt);
             cnt = 0;
             cur = p;
@@ -540,31 +573,31 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
         }
         uint32_t beg, D, j0;
         pair_domain(pr, r, beg, D, j0);
-        for (uint32_t i = lane; i < D; i += 32) {
+        for (uint32_t i = glane; i < D; i += G) {
             A[i] = pr.v.col[beg + i];
             rows[i] = 0;
         }
-        __syncwarp();
-        build_rows_flat<false>(pr.v, pr.asc, A, D, 0, D, s_hb[wib], s_pre[wib], (uint32_t)lane, 32u,
-                               [&](uint32_t i, uint32_t k) {
-                                   atomicOr((unsigned long long *)&rows[i], 1ull << k);
-                                   atomicOr((unsigned long long *)&rows[k], 1ull << i);
-                               });
-        __syncwarp();
+        __syncwarp(gmask);
+        build_rows_flat<G>(pr.v, pr.asc, A, D, 0, D, s_hb[gid], s_pre[gid], (uint32_t)glane, (uint32_t)G, gmask,
+                           [&](uint32_t i, uint32_t k) {
+                               atomicOr((unsigned long long *)&rows[i], 1ull << k);
+                               atomicOr((unsigned long long *)&rows[k], 1ull << i);
+                           });
+        __syncwarp(gmask);
         const uint64_t all = (D >= 64) ? ~0ull : ((1ull << D) - 1ull);
         if constexpr (ENUM) {
             ec.A = A;
             ec.root = r;
         }
-        for (uint32_t j = j0 + lane; j < D; j += 32) {
+        for (uint32_t j = j0 + glane; j < D; j += G) {
             uint32_t x[kMaxQ];
             x[1] = j;
             dfs_thread<2, DEND, ENUM>(pr.lp, rows, all, x, cnt, ec);
         }
-        __syncwarp();
+        __syncwarp(gmask);
     }
-    cnt = warp_sum(cnt);
-    if (lane == 0 && cnt)
+    cnt = group_sum<G>(cnt, gmask);
+    if (glane == 0 && cnt)
         atomicAdd(pr.count, cnt);
 }
 
@@ -616,7 +649,7 @@ __global__ void __launch_bounds__(1024) k_medium(const PairDev *__restrict__ pai
         if (threadIdx.x == 0)
             s_j = j0;
         __syncthreads();
-        build_rows_flat<true>(pr.v, pr.asc, A, D, 0, D, s_hb, s_pre, threadIdx.x, blockDim.x,
+        build_rows_flat<0>(pr.v, pr.asc, A, D, 0, D, s_hb, s_pre, threadIdx.x, blockDim.x, kFull,
                               [&](uint32_t i, uint32_t k) {
                                   atomicOr(&rows[(size_t)i * W + (k >> 5)], 1u << (k & 31));
                                   atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
@@ -701,7 +734,7 @@ __global__ void __launch_bounds__(512) k_large_rows(const PairDev *__restrict__ 
             __syncthreads();
             A = sA;
         }
-        build_rows_flat<true>(pr.v, pr.asc, A, D, i0, i1, s_hb, s_pre, threadIdx.x, blockDim.x,
+        build_rows_flat<0>(pr.v, pr.asc, A, D, i0, i1, s_hb, s_pre, threadIdx.x, blockDim.x, kFull,
                               [&](uint32_t i, uint32_t k) {
                                   atomicOr(&rows[(size_t)i * W + (k >> 5)], 1u << (k & 31));
                                   atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
@@ -776,10 +809,14 @@ __device__ __forceinline__ uint32_t find_pair(const uint64_t *__restrict__ offs,
 // tier[t] for flattened vertex t; dom[t] = its domain size; per tier the
 // largest domain and per (tier, depth) the number of roots.
 __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ offs, uint32_t npairs,
-                           uint64_t N, uint8_t *tier, uint32_t *dom, unsigned *tier_max, unsigned *tier_depth) {
+                           uint64_t N, uint8_t *tier, uint32_t *dom, unsigned *tier_max, unsigned *tier_depth,
+                           unsigned *tiny_depth) {
     __shared__ unsigned s_hist[kTiers * kDepths];
+    __shared__ unsigned s_tiny[kDepths];
     for (int i = threadIdx.x; i < kTiers * kDepths; i += blockDim.x)
         s_hist[i] = 0;
+    for (int i = threadIdx.x; i < kDepths; i += blockDim.x)
+        s_tiny[i] = 0;
     __syncthreads();
     uint32_t mx[kTiers] = {0, 0, 0, 0};
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (uint64_t)gridDim.x * blockDim.x) {
@@ -808,6 +845,8 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
         if (tc) {
             mx[tc - 1] = max(mx[tc - 1], D);
             atomicAdd(&s_hist[(tc - 1) * kDepths + pd.pl.dend], 1u);
+            if (tc == 1 && D <= (uint32_t)kTinyMaxD)
+                atomicAdd(&s_tiny[pd.pl.dend], 1u);
         }
     }
 #pragma unroll
@@ -820,10 +859,13 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
     for (int i = threadIdx.x; i < kTiers * kDepths; i += blockDim.x)
         if (s_hist[i])
             atomicAdd(&tier_depth[i], s_hist[i]);
+    for (int i = threadIdx.x; i < kDepths; i += blockDim.x)
+        if (s_tiny[i])
+            atomicAdd(&tiny_depth[i], s_tiny[i]);
 }
 
-// Selected flattened indices -> items and sort keys: depth, then (medium)
-// largest domain first.
+// Selected flattened indices -> items and sort keys: depth, then (by_domain 1,
+// medium) largest domain first or (by_domain 2, small) smallest first.
 __global__ void k_make_items(const uint32_t *__restrict__ sel, uint32_t ns, const PairDev *__restrict__ pairs,
                              const uint64_t *__restrict__ offs, uint32_t npairs, const uint32_t *__restrict__ dom,
                              int by_domain, uint64_t *items, uint32_t *keys) {
@@ -832,7 +874,8 @@ __global__ void k_make_items(const uint32_t *__restrict__ sel, uint32_t ns, cons
         const uint32_t p = find_pair(offs, npairs, t);
         items[i] = ((uint64_t)p << 32) | (uint64_t)(t - offs[p]);
         const uint32_t dend = (uint32_t)pairs[p].pl.dend;
-        keys[i] = by_domain ? (dend << 16) | (65535u - min(dom[t], 65535u)) : dend;
+        const uint32_t d = min(dom[t], 65535u);
+        keys[i] = by_domain == 1 ? (dend << 16) | (65535u - d) : (by_domain == 2 ? (dend << 16) | d : dend);
     }
 }
 
@@ -898,11 +941,14 @@ struct TierSel {
     }
 
 template <bool ENUM>
-beep_status launch_small(int dend, int grid, cudaStream_t s, const PairDev *pairs, const uint64_t *items,
+beep_status launch_small(int dend, int group, int grid, cudaStream_t s, const PairDev *pairs, const uint64_t *items,
                          uint32_t n) {
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
-        k_small<D, ENUM><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n);                                        \
+        if (group == 8)                                                                                            \
+            k_small<D, ENUM, 8, kTinyMaxD><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n);                      \
+        else                                                                                                       \
+            k_small<D, ENUM, 32, kSmallMaxD><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n);                    \
         break;
     BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
 #undef BEEP_CASE
@@ -997,6 +1043,7 @@ struct Timer {
 struct LaunchRec {
     enum Kind { kSmall, kMedium, kLargeRows, kLargeDfs, kMemset } kind;
     int dend = 0, grid = 0, block = 0;
+    int group = 32; // small tier: lanes per root
     size_t smem = 0;
     const uint64_t *items = nullptr;
     uint32_t n = 0, maxD = 0;
@@ -1135,14 +1182,16 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     BEEP_CUDA_TRY(cudaMemcpyAsync(lp->d_offs, offs.data(), (np + 1) * 8, cudaMemcpyHostToDevice, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(d_misc, 0, 256 * 4, s));
     const int gv = std::max(1, (int)std::min<uint64_t>((N + 255) / 256, (uint64_t)ctx->num_sms * 32));
-    k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, lp->d_tier, d_dom, d_misc, d_misc + 4);
+    k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, lp->d_tier, d_dom, d_misc, d_misc + 4,
+                                  d_misc + 64);
     BEEP_CUDA_TRY(cudaGetLastError());
     st.kernel_launches += 1;
-    unsigned h_misc[64];
+    unsigned h_misc[80];
     BEEP_CUDA_TRY(cudaMemcpyAsync(h_misc, d_misc, sizeof(h_misc), cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     const unsigned *tier_max = h_misc;
     const unsigned *tier_depth = h_misc + 4;
+    const unsigned *tiny_depth = h_misc + 64;
     uint32_t tier_n[kTiers];
     for (int k = 0; k < kTiers; ++k) {
         tier_n[k] = 0;
@@ -1168,7 +1217,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         BEEP_CUDA_TRY(cub::DeviceSelect::If(nullptr, tb, it, d_sel, d_ns, N, sel, s));
         BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
         BEEP_CUDA_TRY(cub::DeviceSelect::If(ctx->scratch.ptr, tb, it, d_sel, d_ns, N, sel, s));
-        const int by_domain = (k == 1 || k == 2) ? 1 : 0;
+        const int by_domain = (k == 1 || k == 2) ? 1 : (k == 0 ? 2 : 0);
         int depths = 0;
         for (int d = 0; d < kDepths; ++d)
             depths += tier_depth[k * kDepths + d] > 0;
@@ -1353,19 +1402,27 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         BEEP_TRY(make_list(0, list));
         uint32_t first = 0;
         for (int d = 3; d < kDepths; ++d) {
-            const uint32_t cnt = tier_depth[d];
-            if (!cnt)
-                continue;
-            LaunchRec r;
-            r.kind = LaunchRec::kSmall;
-            r.dend = d;
-            r.grid = (int)std::min<int64_t>(((int64_t)cnt + kSmallWarps - 1) / kSmallWarps, (int64_t)ctx->num_sms * 8);
-            r.block = kSmallWarps * 32;
-            r.items = list + first;
-            r.n = cnt;
-            r.sink = &st.small_ms;
-            lp->recs.push_back(r);
-            first += cnt;
+            // the list is sorted by (depth, domain): tiny domains first
+            const uint32_t n_tiny = tiny_depth[d], n_rest = tier_depth[d] - tiny_depth[d];
+            for (int part = 0; part < 2; ++part) {
+                const uint32_t cnt = part == 0 ? n_tiny : n_rest;
+                if (!cnt)
+                    continue;
+                const int group = part == 0 ? 8 : 32;
+                const int per_block = kSmallWarps * 32 / group;
+                LaunchRec r;
+                r.kind = LaunchRec::kSmall;
+                r.dend = d;
+                r.group = group;
+                r.grid = (int)std::min<int64_t>(((int64_t)cnt + per_block - 1) / per_block,
+                                                (int64_t)ctx->num_sms * 8);
+                r.block = kSmallWarps * 32;
+                r.items = list + first;
+                r.n = cnt;
+                r.sink = &st.small_ms;
+                lp->recs.push_back(r);
+                first += cnt;
+            }
         }
     }
     // shared-memory opt-ins are host calls: done here, never inside a capture
@@ -1454,9 +1511,9 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::ve
             break;
         case LaunchRec::kSmall:
             if (lp->enumerate)
-                BEEP_TRY(launch_small<true>(r.dend, r.grid, rs, lp->d_pairs, r.items, r.n));
+                BEEP_TRY(launch_small<true>(r.dend, r.group, r.grid, rs, lp->d_pairs, r.items, r.n));
             else
-                BEEP_TRY(launch_small<false>(r.dend, r.grid, rs, lp->d_pairs, r.items, r.n));
+                BEEP_TRY(launch_small<false>(r.dend, r.group, r.grid, rs, lp->d_pairs, r.items, r.n));
             st.small_launches++;
             break;
         }
