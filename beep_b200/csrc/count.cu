@@ -133,23 +133,6 @@ __device__ __forceinline__ uint32_t free_count_rootonly(uint32_t D, const uint32
     return A;
 }
 
-// Domain of root r: list A = col[beg, beg + D); level-1 index starts at j0.
-__device__ __forceinline__ void root_domain(const ViewDev &v, const DevPlan &pl, uint32_t r, uint32_t &beg,
-                                            uint32_t &D, uint32_t &j0) {
-    const uint32_t b = v.rp[r], e = v.rp[r + 1], sp = v.split[r];
-    if (pl.restricted) {
-        beg = b + sp;
-        D = e - b - sp;
-        j0 = 0;
-    } else {
-        beg = b;
-        D = e - b;
-        // position 1 symmetric to the root: only neighbours after the root
-        // (sgm_kernelsLD.cuh:60)
-        j0 = pl.pos1_after_root ? sp : 0;
-    }
-}
-
 // Higher-priority list of u and the part of A it can meet.
 __device__ __forceinline__ void hd_range(const ViewDev &v, int asc, uint32_t u, uint32_t i, uint32_t D,
                                          uint32_t &hb, uint32_t &he, uint32_t &xb, uint32_t &xe) {
@@ -230,9 +213,11 @@ __device__ __forceinline__ void emit_bits(const EnumCtx &ec, const uint32_t (&x)
 // ---------------------------------------------------------------------------
 // thread-level DFS on 64-bit rows (D <= 64)
 // ---------------------------------------------------------------------------
+// rows[i - rlo] is the row of domain vertex i (only rows i >= rlo exist; the
+// plan reads no other).
 template <int P, int DEND, bool ENUM>
-__device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, uint64_t all, uint32_t (&x)[kMaxQ],
-                                           unsigned long long &cnt, const EnumCtx &ec) {
+__device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, uint32_t rlo, uint64_t all,
+                                           uint32_t (&x)[kMaxQ], unsigned long long &cnt, const EnumCtx &ec) {
     bool closed = false; // count this level's candidates as C(A, DEND - P)
     if constexpr (!ENUM && DEND - P <= 4) {
         const uint32_t lo = level_bound<P>(lp, x);
@@ -249,7 +234,7 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
 #pragma unroll
     for (int q = 1; q < P; ++q) {
         if (bk >> q & 1u)
-            c &= rows[x[q]];
+            c &= rows[x[q] - rlo];
         c &= ~(1ull << x[q]);
         if (sy >> q & 1u)
             c &= ~((2ull << x[q]) - 1ull); // keep bits above x[q]
@@ -267,7 +252,7 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
             const int b = __ffsll((long long)c) - 1;
             c &= c - 1;
             x[P] = (uint32_t)b;
-            dfs_thread<P + 1, DEND, ENUM>(lp, rows, all, x, cnt, ec);
+            dfs_thread<P + 1, DEND, ENUM>(lp, rows, rlo, all, x, cnt, ec);
         }
     }
 }
@@ -275,34 +260,42 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
 // ---------------------------------------------------------------------------
 // warp-level DFS on rows of W 32-bit words (lane k holds word k of a chunk)
 // ---------------------------------------------------------------------------
-template <int P, int DEND, bool ENUM>
-__device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint32_t W, uint32_t D,
-                                         uint32_t (&x)[kMaxQ], unsigned long long &cnt, int lane, const EnumCtx &ec) {
+// bm + (i - rlo) * W is the row of domain vertex i (rows i >= rlo only).
+// A group of G lanes (G = 32: a warp; gmask its lanes, glane the lane within
+// it) walks the words of a level G at a time; every lane of the group calls
+// this together.
+template <int P, int DEND, bool ENUM, int G = 32>
+__device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint32_t rlo, uint32_t W, uint32_t D,
+                                         uint32_t (&x)[kMaxQ], unsigned long long &cnt, int glane, const EnumCtx &ec,
+                                         unsigned gmask = kFull) {
+    constexpr int LG = G == 32 ? 5 : (G == 16 ? 4 : (G == 8 ? 3 : (G == 4 ? 2 : (G == 2 ? 1 : 0))));
+    static_assert((1 << LG) == G, "group size must be a power of two up to 32");
     const uint32_t bk = lp.back[P];
     const uint32_t lo = level_bound<P>(lp, x);
-    bool closed = false; // warp-uniform: count this level's candidates as C(A, DEND - P)
+    bool closed = false; // group-uniform: count this level's candidates as C(A, DEND - P)
     if constexpr (!ENUM && DEND - P <= 4) {
         if (suffix_applies<P, DEND>(lp, x, lo)) {
             if (lp.free_back == 0) {
-                if (lane == 0)
+                if (glane == 0)
                     cnt += binom_le4(free_count_rootonly<P>(D, x, lo), DEND - P);
                 return;
             }
             closed = true;
         }
     }
+    const int gbase = (threadIdx.x & 31) & ~(G - 1);
     uint32_t acc = 0;
-    const uint32_t nch = (W + 31) >> 5;
+    const uint32_t nch = (W + G - 1) >> LG;
     const uint32_t tail = D & 31;
-    for (uint32_t ch = lo >> 10; ch < nch; ++ch) {
-        const uint32_t k = (ch << 5) + lane;
+    for (uint32_t ch = lo >> (5 + LG); ch < nch; ++ch) {
+        const uint32_t k = (ch << LG) + glane;
         uint32_t w = 0;
         if (k < W) {
             w = (k + 1 < W || tail == 0) ? kFull : ((1u << tail) - 1u);
 #pragma unroll
             for (int q = 1; q < P; ++q) {
                 if (bk >> q & 1u)
-                    w &= bm[(size_t)x[q] * W + k];
+                    w &= bm[(size_t)(x[q] - rlo) * W + k];
                 if ((x[q] >> 5) == k)
                     w &= ~(1u << (x[q] & 31));
             }
@@ -321,22 +314,29 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
                 emit_bits(ec, x, P, (uint64_t)w, k << 5);
             cnt += (unsigned long long)__popc(w);
         } else {
-            unsigned bal = __ballot_sync(kFull, w != 0);
+            unsigned bal = __ballot_sync(gmask, w != 0) >> gbase;
+            if constexpr (G < 32)
+                bal &= (1u << G) - 1u;
             while (bal) {
                 const int L = __ffs(bal) - 1;
-                const uint32_t ww = __shfl_sync(kFull, w, L);
+                const uint32_t ww = __shfl_sync(gmask, w, L, G);
                 const int b = __ffs(ww) - 1;
-                if (lane == L)
+                if (glane == L)
                     w &= w - 1;
-                x[P] = (((ch << 5) + (uint32_t)L) << 5) + (uint32_t)b;
-                dfs_warp<P + 1, DEND, ENUM>(lp, bm, W, D, x, cnt, lane, ec);
-                bal = __ballot_sync(kFull, w != 0);
+                x[P] = (((ch << LG) + (uint32_t)L) << 5) + (uint32_t)b;
+                dfs_warp<P + 1, DEND, ENUM, G>(lp, bm, rlo, W, D, x, cnt, glane, ec, gmask);
+                bal = __ballot_sync(gmask, w != 0) >> gbase;
+                if constexpr (G < 32)
+                    bal &= (1u << G) - 1u;
             }
         }
     }
     if (closed) {
-        const uint32_t A = __reduce_add_sync(kFull, acc);
-        if (lane == 0)
+        uint32_t A = acc;
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1)
+            A += __shfl_xor_sync(gmask, A, o, G);
+        if (glane == 0)
             cnt += binom_le4(A, DEND - P);
     }
 }
@@ -422,15 +422,23 @@ template <int G> __device__ __forceinline__ void group_sync(unsigned gmask) {
 // costs fewer dependent loads.
 constexpr uint32_t kTrimMin = 16;
 
+// Only edges with an endpoint at index >= rlo are found (the rows below rlo
+// are not stored): in ascending order row i searches A[max(i + 1, rlo), D),
+// in descending order rows below rlo search nothing.
 template <int G, typename SetFn>
 __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const uint32_t *A, uint32_t D,
-                                                uint32_t i0, uint32_t i1, uint32_t *s_hb, uint32_t *s_pre,
-                                                uint32_t tid, uint32_t nthr, unsigned gmask, SetFn set) {
+                                                uint32_t rlo, uint32_t i0, uint32_t i1, uint32_t *s_hb,
+                                                uint32_t *s_pre, uint32_t tid, uint32_t nthr, unsigned gmask,
+                                                SetFn set) {
     const uint32_t R = i1 - i0;
     for (uint32_t r = tid; r < R; r += nthr) {
         const uint32_t i = i0 + r;
         uint32_t hb, he, xb, xe, c = 0;
         hd_range(v, asc, A[i], i, D, hb, he, xb, xe);
+        if (asc)
+            xb = max(xb, rlo);
+        else if (i < rlo)
+            xe = 0;
         if (xb < xe && hb < he) {
             if (he - hb > kTrimMin) {
                 const uint32_t lo = lower_bound_g(v.col, hb, he, A[xb]);
@@ -465,7 +473,7 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
         }
         const uint32_t i = i0 + lo;
         const uint32_t w = v.col[s_hb[lo] + (t - s_pre[lo])];
-        const uint32_t xb = asc ? i + 1 : 0, xe = asc ? D : i;
+        const uint32_t xb = asc ? max(i + 1, rlo) : 0, xe = asc ? D : i;
         const int k = find_idx(A, xb, xe, w);
         if (k >= 0)
             set(i, (uint32_t)k);
@@ -496,7 +504,7 @@ __device__ __forceinline__ uint32_t item_root(uint64_t it) { return (uint32_t)it
 struct PairRegs {
     ViewDev v;
     Lp lp;
-    int restricted, pos1, asc;
+    int restricted, pos1, asc, rows_needed;
     unsigned long long *count;
 };
 
@@ -507,6 +515,7 @@ __device__ __forceinline__ void load_pair(const PairDev *__restrict__ pairs, uin
     pr.restricted = pd.pl.restricted;
     pr.pos1 = pd.pl.pos1_after_root;
     pr.asc = pd.pl.asc;
+    pr.rows_needed = pd.pl.rows_needed;
     pr.count = pd.count;
 }
 
@@ -524,6 +533,12 @@ __device__ __forceinline__ void pair_domain(const PairRegs &pr, uint32_t r, uint
         // (sgm_kernelsLD.cuh:60)
         j0 = pr.pos1 ? sp : 0;
     }
+}
+
+// First stored row of a root's bitmap: the plan reads the rows of level-1
+// candidates only (j0), none (D) or all (0).
+__device__ __forceinline__ uint32_t pair_rlo(const PairRegs &pr, uint32_t D, uint32_t j0) {
+    return pr.rows_needed == 2 ? 0u : (pr.rows_needed == 1 ? j0 : D);
 }
 
 // ---------------------------------------------------------------------------
@@ -573,16 +588,20 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
         }
         uint32_t beg, D, j0;
         pair_domain(pr, r, beg, D, j0);
+        const uint32_t rlo = pair_rlo(pr, D, j0);
         for (uint32_t i = glane; i < D; i += G) {
             A[i] = pr.v.col[beg + i];
             rows[i] = 0;
         }
         __syncwarp(gmask);
-        build_rows_flat<G>(pr.v, pr.asc, A, D, 0, D, s_hb[gid], s_pre[gid], (uint32_t)glane, (uint32_t)G, gmask,
-                           [&](uint32_t i, uint32_t k) {
-                               atomicOr((unsigned long long *)&rows[i], 1ull << k);
-                               atomicOr((unsigned long long *)&rows[k], 1ull << i);
-                           });
+        if (rlo < D)
+            build_rows_flat<G>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb[gid], s_pre[gid], (uint32_t)glane, (uint32_t)G,
+                               gmask, [&](uint32_t i, uint32_t k) {
+                                   if (i >= rlo)
+                                       atomicOr((unsigned long long *)&rows[i - rlo], 1ull << k);
+                                   if (k >= rlo)
+                                       atomicOr((unsigned long long *)&rows[k - rlo], 1ull << i);
+                               });
         __syncwarp(gmask);
         const uint64_t all = (D >= 64) ? ~0ull : ((1ull << D) - 1ull);
         if constexpr (ENUM) {
@@ -592,7 +611,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
         for (uint32_t j = j0 + glane; j < D; j += G) {
             uint32_t x[kMaxQ];
             x[1] = j;
-            dfs_thread<2, DEND, ENUM>(pr.lp, rows, all, x, cnt, ec);
+            dfs_thread<2, DEND, ENUM>(pr.lp, rows, rlo, all, x, cnt, ec);
         }
         __syncwarp(gmask);
     }
@@ -604,7 +623,9 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
 // ---------------------------------------------------------------------------
 // medium tier: block per root, bitmap in shared memory
 // ---------------------------------------------------------------------------
-template <int DEND, bool ENUM>
+// G lanes per level-1 vertex: 8 for domains of at most 256 vertices (rows of
+// at most 8 words), 32 above.
+template <int DEND, bool ENUM, int G>
 __global__ void __launch_bounds__(1024) k_medium(const PairDev *__restrict__ pairs,
                                                 const uint64_t *__restrict__ items, uint32_t nitems,
                                                 unsigned *cursor, uint32_t maxD) {
@@ -641,34 +662,40 @@ __global__ void __launch_bounds__(1024) k_medium(const PairDev *__restrict__ pai
         }
         uint32_t beg, D, j0;
         pair_domain(pr, r, beg, D, j0);
+        const uint32_t rlo = pair_rlo(pr, D, j0);
         const uint32_t W = (D + 31) >> 5;
         for (uint32_t i = threadIdx.x; i < D; i += blockDim.x)
             A[i] = pr.v.col[beg + i];
-        for (uint32_t i = threadIdx.x; i < D * W; i += blockDim.x)
+        for (uint32_t i = threadIdx.x; i < (D - rlo) * W; i += blockDim.x)
             rows[i] = 0;
         if (threadIdx.x == 0)
             s_j = j0;
         __syncthreads();
-        build_rows_flat<0>(pr.v, pr.asc, A, D, 0, D, s_hb, s_pre, threadIdx.x, blockDim.x, kFull,
-                              [&](uint32_t i, uint32_t k) {
-                                  atomicOr(&rows[(size_t)i * W + (k >> 5)], 1u << (k & 31));
-                                  atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
-                              });
+        if (rlo < D) // block-uniform
+            build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, threadIdx.x, blockDim.x, kFull,
+                               [&](uint32_t i, uint32_t k) {
+                                   if (i >= rlo)
+                                       atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
+                                   if (k >= rlo)
+                                       atomicOr(&rows[(size_t)(k - rlo) * W + (i >> 5)], 1u << (i & 31));
+                               });
         __syncthreads();
         if constexpr (ENUM) {
             ec.A = A;
             ec.root = r;
         }
+        const int glane = lane & (G - 1);
+        const unsigned gmask = G == 32 ? kFull : (((1u << G) - 1u) << (lane & ~(G - 1)));
         for (;;) {
             uint32_t j = 0;
-            if (lane == 0)
+            if (glane == 0)
                 j = atomicAdd(&s_j, 1u);
-            j = __shfl_sync(kFull, j, 0);
+            j = __shfl_sync(gmask, j, 0, G);
             if (j >= D)
                 break;
             uint32_t x[kMaxQ];
             x[1] = j;
-            dfs_warp<2, DEND, ENUM>(pr.lp, rows, W, D, x, cnt, lane, ec);
+            dfs_warp<2, DEND, ENUM, G>(pr.lp, rows, rlo, W, D, x, cnt, glane, ec, gmask);
         }
         __syncthreads();
     }
@@ -723,6 +750,7 @@ __global__ void __launch_bounds__(512) k_large_rows(const PairDev *__restrict__ 
         load_pair(pairs, item_pair(it), pr);
         uint32_t beg, D, j0;
         pair_domain(pr, item_root(it), beg, D, j0);
+        const uint32_t rlo = pair_rlo(pr, D, j0);
         const uint32_t W = (D + 31) >> 5;
         uint32_t *rows = arena + bt.off[b];
         const uint32_t i0 = (c - bt.cstart[b]) * kRowsPerChunk;
@@ -734,11 +762,14 @@ __global__ void __launch_bounds__(512) k_large_rows(const PairDev *__restrict__ 
             __syncthreads();
             A = sA;
         }
-        build_rows_flat<0>(pr.v, pr.asc, A, D, i0, i1, s_hb, s_pre, threadIdx.x, blockDim.x, kFull,
-                              [&](uint32_t i, uint32_t k) {
-                                  atomicOr(&rows[(size_t)i * W + (k >> 5)], 1u << (k & 31));
-                                  atomicOr(&rows[(size_t)k * W + (i >> 5)], 1u << (i & 31));
-                              });
+        if (rlo < D) // block-uniform
+            build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, i0, i1, s_hb, s_pre, threadIdx.x, blockDim.x, kFull,
+                               [&](uint32_t i, uint32_t k) {
+                                   if (i >= rlo)
+                                       atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
+                                   if (k >= rlo)
+                                       atomicOr(&rows[(size_t)(k - rlo) * W + (i >> 5)], 1u << (i & 31));
+                               });
         __syncthreads();
     }
 }
@@ -781,7 +812,7 @@ __global__ void __launch_bounds__(256) k_large_dfs(const PairDev *__restrict__ p
         }
         uint32_t x[kMaxQ];
         x[1] = j0 + (t - bt.tstart[b]);
-        dfs_warp<2, DEND, ENUM>(pr.lp, arena + bt.off[b], W, D, x, cnt, lane, ec);
+        dfs_warp<2, DEND, ENUM>(pr.lp, arena + bt.off[b], pair_rlo(pr, D, j0), W, D, x, cnt, lane, ec);
     }
     cnt = warp_sum(cnt);
     if (lane == 0 && cnt)
@@ -957,21 +988,8 @@ beep_status launch_small(int dend, int group, int grid, cudaStream_t s, const Pa
 }
 
 template <int D, bool ENUM> beep_status set_medium_attr(size_t smem) {
-    BEEP_CUDA_TRY(cudaFuncSetAttribute(k_medium<D, ENUM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    return BEEP_OK;
-}
-
-template <bool ENUM>
-beep_status launch_medium(int dend, int grid, int block, size_t smem, cudaStream_t s, const PairDev *pairs,
-                          const uint64_t *items, uint32_t n, unsigned *cursor, uint32_t maxD) {
-#define BEEP_CASE(D)                                                                                               \
-    case D:                                                                                                        \
-        BEEP_TRY((set_medium_attr<D, ENUM>(smem)));                                                                \
-        k_medium<D, ENUM><<<grid, block, smem, s>>>(pairs, items, n, cursor, maxD);                                 \
-        break;
-    BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
-#undef BEEP_CASE
-    BEEP_CUDA_TRY(cudaGetLastError());
+    BEEP_CUDA_TRY(cudaFuncSetAttribute(k_medium<D, ENUM, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BEEP_CUDA_TRY(cudaFuncSetAttribute(k_medium<D, ENUM, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     return BEEP_OK;
 }
 
@@ -1256,10 +1274,15 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         struct R {
             uint64_t item;
             uint32_t D, j0, dend;
+            uint64_t words; // bitmap rows [rlo, D) of D bits, rounded up to 32 words
         };
         std::vector<R> rs(nl);
-        for (uint32_t i = 0; i < nl; ++i)
-            rs[i] = R{litems[i], lD[i], lj[i], (uint32_t)hp[(uint32_t)(litems[i] >> 32)].pl.dend};
+        for (uint32_t i = 0; i < nl; ++i) {
+            const DevPlan &pl = hp[(uint32_t)(litems[i] >> 32)].pl;
+            const uint32_t D = lD[i], rlo = pl.rows_needed == 2 ? 0u : (pl.rows_needed == 1 ? lj[i] : D);
+            const uint64_t words = ((uint64_t)(D - rlo) * ((D + 31) / 32) + 31) & ~(uint64_t)31;
+            rs[i] = R{litems[i], D, lj[i], (uint32_t)pl.dend, words};
+        }
         std::sort(rs.begin(), rs.end(), [](const R &a, const R &b) { return a.D > b.D; });
         size_t free_b = 0, total_b = 0;
         BEEP_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
@@ -1270,7 +1293,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         for (size_t i0 = 0; i0 < rs.size();) {
             size_t words = 0, i1 = i0;
             while (i1 < rs.size()) {
-                const uint64_t w = ((uint64_t)rs[i1].D * ((rs[i1].D + 31) / 32) + 31) & ~(uint64_t)31;
+                const uint64_t w = rs[i1].words;
                 if (i1 > i0 && (words + w) * 4 > arena_cap)
                     break;
                 words += w;
@@ -1299,7 +1322,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             for (size_t i = i0; i < i1; ++i) {
                 bitem.push_back(rs[i].item);
                 boff.push_back(words);
-                words += ((uint64_t)rs[i].D * ((rs[i].D + 31) / 32) + 31) & ~(uint64_t)31;
+                words += rs[i].words;
                 cstart.push_back(cstart.back() + (rs[i].D + kRowsPerChunk - 1) / kRowsPerChunk);
             }
             std::vector<std::pair<uint32_t, uint32_t>> groups; // (first entry, count) per depth
@@ -1384,6 +1407,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             LaunchRec r;
             r.kind = LaunchRec::kMedium;
             r.dend = d;
+            r.group = sub == 0 ? 8 : 32;
             r.grid = ctx->num_sms * per_sm;
             r.block = block;
             r.smem = smem;
@@ -1499,10 +1523,14 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::ve
         case LaunchRec::kMedium:
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
-        if (lp->enumerate)                                                                                         \
-            k_medium<D, true><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);       \
+        if (lp->enumerate && r.group == 8)                                                                         \
+            k_medium<D, true, 8><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);    \
+        else if (lp->enumerate)                                                                                    \
+            k_medium<D, true, 32><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);   \
+        else if (r.group == 8)                                                                                     \
+            k_medium<D, false, 8><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);   \
         else                                                                                                       \
-            k_medium<D, false><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);      \
+            k_medium<D, false, 32><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);  \
         break;
             BEEP_DEPTH_SWITCH(r.dend, BEEP_CASE)
 #undef BEEP_CASE
@@ -1878,7 +1906,7 @@ __global__ void __launch_bounds__(512) k_noalloc_count(const uint32_t *__restric
                     break;
                 uint32_t x[kMaxQ];
                 x[1] = j;
-                dfs_warp<2, DEND, false>(lp, rows, W, D, x, cnt, lane, ec);
+                dfs_warp<2, DEND, false>(lp, rows, 0u, W, D, x, cnt, lane, ec);
             }
         }
         __syncthreads();

@@ -69,7 +69,7 @@ struct DevPlan {
     int32_t asc;             // ascending (degree, id) priority order
     int32_t free_from;       // positions [free_from, dend) share one back-edge set and form a symmetry chain
     uint32_t free_back;      // that back-edge set (bits q >= 1; 0: only the root)
-    int32_t pad2;
+    int32_t rows_needed;     // adjacency rows the DFS reads: 0 none, 1 only position 1's, 2 any
 };
 
 struct QueryPlan {

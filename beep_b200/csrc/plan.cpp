@@ -255,6 +255,13 @@ beep_status compile_plan(int32_t qn, const std::vector<int32_t> &rp, const std::
             D.free_from = p;
         }
     }
+    // Rows the DFS reads: those of the positions that are back edges of a
+    // later position. When that is position 1 alone, only the rows of the
+    // level-1 candidates are built.
+    uint32_t read = 0;
+    for (int p = 2; p < D.dend; ++p)
+        read |= D.back[p];
+    D.rows_needed = read == 0 ? 0 : (read == 2u ? 1 : 2);
     out->info = P;
     out->dev = D;
     return BEEP_OK;
