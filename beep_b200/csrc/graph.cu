@@ -273,14 +273,78 @@ __global__ void k_prio_keys(const uint32_t *__restrict__ deg, int64_t n, uint32_
         atomicAdd(n_alive, c);
 }
 
+// Rows of at most kSortShort entries are sorted by k_sort_short; longer ones
+// are listed here for a segmented sort.
+constexpr uint32_t kSortShort = 32;
+
 __global__ void k_rank(const uint64_t *__restrict__ keys, int64_t n_alive, uint32_t *orig, uint32_t *rank,
-                       const uint32_t *__restrict__ deg, uint32_t *new_deg) {
+                       const uint32_t *__restrict__ deg, uint32_t *new_deg, uint32_t *long_rows,
+                       unsigned *n_long) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_alive;
          i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t v = (uint32_t)keys[i];
+        const uint32_t d = deg[v];
         orig[i] = v;
         rank[v] = (uint32_t)i;
-        new_deg[i] = deg[v];
+        new_deg[i] = d;
+        if (d > kSortShort)
+            long_rows[atomicAdd(n_long, 1u)] = (uint32_t)i;
+    }
+}
+
+__global__ void k_long_offsets(const uint32_t *__restrict__ long_rows, const unsigned *__restrict__ n_long,
+                               const uint32_t *__restrict__ rp, uint32_t *beg, uint32_t *end) {
+    const uint32_t nl = *n_long;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nl; k += gridDim.x * blockDim.x) {
+        const uint32_t i = long_rows[k];
+        beg[k] = rp[i];
+        end[k] = rp[i + 1];
+    }
+}
+
+// Ascending bitonic sort of one value per lane across a group of G lanes.
+template <int G> __device__ __forceinline__ uint32_t bitonic_sort(uint32_t x, int glane) {
+#pragma unroll
+    for (int k = 2; k <= G; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t y = __shfl_xor_sync(kFull, x, j, G);
+            x = (((glane & j) == 0) == ((glane & k) == 0)) ? min(x, y) : max(x, y);
+        }
+    return x;
+}
+
+// Sorts the rows of at most kSortShort entries from `in` into `out` (same
+// offsets). A warp takes four rows: when all four have at most 8 entries each
+// 8-lane group sorts one, otherwise the warp sorts them one after the other.
+__global__ void k_sort_short(const uint32_t *__restrict__ rp, int64_t n, const uint32_t *__restrict__ in,
+                             uint32_t *out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; base < n; base += warps * 4) {
+        const int64_t my = base + (lane >> 3);
+        uint32_t b = 0, L = 0;
+        if (my < n) {
+            b = rp[my];
+            L = rp[my + 1] - b;
+        }
+        if (__all_sync(kFull, L <= 8)) {
+            const int g = lane & 7;
+            uint32_t x = (uint32_t)g < L ? in[b + g] : 0xffffffffu;
+            x = bitonic_sort<8>(x, g);
+            if ((uint32_t)g < L)
+                out[b + g] = x;
+        } else {
+            for (int r = 0; r < 4; ++r) {
+                const uint32_t rb = __shfl_sync(kFull, b, r * 8), rl = __shfl_sync(kFull, L, r * 8);
+                if (rl > kSortShort) // warp-uniform
+                    continue;
+                uint32_t x = (uint32_t)lane < rl ? in[rb + lane] : 0xffffffffu;
+                x = bitonic_sort<32>(x, lane);
+                if ((uint32_t)lane < rl)
+                    out[rb + lane] = x;
+            }
+        }
     }
 }
 
@@ -578,7 +642,8 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     const int64_t nn = n > 0 ? n : 1;
     const size_t cap = chunk_capacity(n, m);
     size_t need = Carve::need({(size_t)nn * 4, (size_t)nn, (size_t)nn * 4, (size_t)nn * 8, (size_t)nn * 8,
-                               (size_t)nn * 4, (size_t)(m > 0 ? m : 1) * 4, cap * sizeof(RowChunk), 16});
+                               (size_t)nn * 4, (size_t)(m > 0 ? m : 1) * 4, cap * sizeof(RowChunk), 16,
+                               (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4});
     BEEP_TRY(ctx->grow(ctx->scratch2, need));
     Carve cv(ctx->scratch2.ptr);
     uint32_t *deg = cv.take<uint32_t>(nn);
@@ -589,7 +654,10 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     uint32_t *new_deg = cv.take<uint32_t>(nn);
     uint32_t *col_tmp = cv.take<uint32_t>(m > 0 ? m : 1);
     RowChunk *chunks = cv.take<RowChunk>(cap);
-    unsigned *d_nchunks = cv.take<unsigned>(4);
+    unsigned *d_nchunks = cv.take<unsigned>(4); // [0] chunks, [1] long rows
+    uint32_t *long_rows = cv.take<uint32_t>(nn);
+    uint32_t *long_beg = cv.take<uint32_t>(nn);
+    uint32_t *long_end = cv.take<uint32_t>(nn);
     const uint32_t ucap = (uint32_t)std::min<size_t>(cap, 0xffffffffu);
     BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned long long *d_removed = ctx->counter.as<unsigned long long>();
@@ -656,9 +724,10 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_TRY(ctx->grow(v->split, (size_t)(na > 0 ? na : 1) * 4));
     BEEP_CUDA_TRY(cudaMemsetAsync(rank, 0xff, (size_t)nn * 4, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(new_deg, 0, (size_t)nn * 4, s));
+    BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks + 1, 0, 4, s));
     if (na > 0) {
         k_rank<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(keys2, na, v->orig.as<uint32_t>(), rank, deg,
-                                                               new_deg);
+                                                               new_deg, long_rows, d_nchunks + 1);
         ++ctx->launches;
     }
     BEEP_CUDA_TRY(cudaGetLastError());
@@ -667,9 +736,11 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, new_deg, nrp, na + 1, s));
     BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ctx->scratch.ptr, tb, new_deg, nrp, na + 1, s));
-    uint32_t h_m = 0;
-    BEEP_CUDA_TRY(cudaMemcpyAsync(&h_m, nrp + na, 4, cudaMemcpyDeviceToHost, s));
+    uint32_t *h2 = reinterpret_cast<uint32_t *>(ctx->h_pinned);
+    BEEP_CUDA_TRY(cudaMemcpyAsync(h2, nrp + na, 4, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaMemcpyAsync(h2 + 1, d_nchunks + 1, 4, cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    const uint32_t h_m = h2[0], n_long = h2[1];
     v->m = h_m;
     tr.mark("rank_scan");
     BEEP_TRY(ctx->grow(v->col, (size_t)(h_m > 0 ? h_m : 1) * 4));
@@ -683,13 +754,25 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     }
     BEEP_CUDA_TRY(cudaGetLastError());
     tr.mark("fill");
-    if (h_m > 0) {
+    // Sort every row: short rows by warps, the long ones by a segmented sort
+    // over their segments only (CUB leaves keys outside the segments alone).
+    if (na > 0 && h_m > 0) {
+        k_sort_short<<<grid_for((na + 3) / 4 * 32, 256, ctx->num_sms), 256, 0, s>>>(nrp, na, col_tmp,
+                                                                                 v->col.as<uint32_t>());
+        ++ctx->launches;
+        BEEP_CUDA_TRY(cudaGetLastError());
+    }
+    if (n_long > 0) {
+        k_long_offsets<<<grid_for(n_long, 256, ctx->num_sms), 256, 0, s>>>(long_rows, d_nchunks + 1, nrp,
+                                                                           long_beg, long_end);
+        ++ctx->launches;
+        BEEP_CUDA_TRY(cudaGetLastError());
         tb = 0;
         BEEP_CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(nullptr, tb, col_tmp, v->col.as<uint32_t>(), (int64_t)h_m,
-                                                         na, nrp, nrp + 1, s));
+                                                         (int64_t)n_long, long_beg, long_end, s));
         BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
         BEEP_CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(ctx->scratch.ptr, tb, col_tmp, v->col.as<uint32_t>(),
-                                                         (int64_t)h_m, na, nrp, nrp + 1, s));
+                                                         (int64_t)h_m, (int64_t)n_long, long_beg, long_end, s));
     }
     if (na > 0) {
         k_split<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(nrp, v->col.as<uint32_t>(), na,
