@@ -162,7 +162,22 @@ __device__ __forceinline__ uint32_t lower_bound_g(const uint32_t *__restrict__ a
     return lo;
 }
 
-// Index of key in sorted a[lo, hi) or -1.
+// Whether sorted a[lo, hi) holds key.
+__device__ __forceinline__ bool contains_g(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi, uint32_t key) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t x = a[mid];
+        if (x == key)
+            return true;
+        if (x < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return false;
+}
+
+// Index of key in sorted a[lo, hi) or -1 (a holds fewer than 2^31 entries).
 __device__ __forceinline__ int find_idx(const uint32_t *a, uint32_t lo, uint32_t hi, uint32_t key) {
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
@@ -422,18 +437,30 @@ template <int G> __device__ __forceinline__ void group_sync(unsigned gmask) {
 // costs fewer dependent loads.
 constexpr uint32_t kTrimMin = 16;
 
+// floor(log2(x)) + 1 for x >= 1 (the steps of a binary search over x entries)
+__device__ __forceinline__ uint32_t search_steps(uint32_t x) { return 32u - (uint32_t)__clz(x | 1u); }
+
 // Only edges with an endpoint at index >= rlo are found (the rows below rlo
 // are not stored): in ascending order row i searches A[max(i + 1, rlo), D),
 // in descending order rows below rlo search nothing.
+//
+// Each row picks the cheaper direction: its list slice (c entries) searched
+// in A (shared memory, c * log D steps), or the nA entries of A it can meet
+// searched in the list slice (global memory, nA * log c steps) when the
+// slice is much longer than that part of A -- the usual case for domain
+// vertices of high degree. s_len[r] holds the slice length, with the top bit
+// set for the second direction.
 template <int G, typename SetFn>
 __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const uint32_t *A, uint32_t D,
                                                 uint32_t rlo, uint32_t i0, uint32_t i1, uint32_t *s_hb,
-                                                uint32_t *s_pre, uint32_t tid, uint32_t nthr, unsigned gmask,
-                                                SetFn set) {
+                                                uint32_t *s_pre, uint32_t *s_len, uint32_t tid, uint32_t nthr,
+                                                unsigned gmask, SetFn set) {
+    constexpr uint32_t kByA = 0x80000000u;
     const uint32_t R = i1 - i0;
+    const uint32_t logD = search_steps(D);
     for (uint32_t r = tid; r < R; r += nthr) {
         const uint32_t i = i0 + r;
-        uint32_t hb, he, xb, xe, c = 0;
+        uint32_t hb, he, xb, xe, c = 0, work = 0, len = 0;
         hd_range(v, asc, A[i], i, D, hb, he, xb, xe);
         if (asc)
             xb = max(xb, rlo);
@@ -448,9 +475,17 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
             } else {
                 c = he - hb;
             }
+            const uint32_t nA = xe - xb;
+            len = c;
+            work = c;
+            if (c > 0 && c < kByA && (uint64_t)nA * search_steps(c) * 2 < (uint64_t)c * logD) {
+                len = c | kByA;
+                work = nA;
+            }
         }
         s_hb[r] = hb;
-        s_pre[r] = c;
+        s_len[r] = len;
+        s_pre[r] = work;
     }
     group_sync<G>(gmask);
     if constexpr (G == 0) {
@@ -472,11 +507,19 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
                 hi = mid;
         }
         const uint32_t i = i0 + lo;
-        const uint32_t w = v.col[s_hb[lo] + (t - s_pre[lo])];
+        const uint32_t len = s_len[lo];
         const uint32_t xb = asc ? max(i + 1, rlo) : 0, xe = asc ? D : i;
-        const int k = find_idx(A, xb, xe, w);
-        if (k >= 0)
-            set(i, (uint32_t)k);
+        if (len & kByA) {
+            const uint32_t k = xb + (t - s_pre[lo]);
+            const uint32_t hb = s_hb[lo];
+            if (contains_g(v.col, hb, hb + (len & ~kByA), A[k]))
+                set(i, k);
+        } else {
+            const uint32_t w = v.col[s_hb[lo] + (t - s_pre[lo])];
+            const int k = find_idx(A, xb, xe, w);
+            if (k >= 0)
+                set(i, (uint32_t)k);
+        }
     }
 }
 
@@ -563,6 +606,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
     __shared__ uint64_t s_rows[NG][MAXD];
     __shared__ uint32_t s_A[NG][MAXD];
     __shared__ uint32_t s_hb[NG][MAXD];
+    __shared__ uint32_t s_len[NG][MAXD];
     __shared__ uint32_t s_pre[NG][MAXD + 1];
     const int gid = threadIdx.x / G, glane = threadIdx.x % G;
     const int lane = threadIdx.x & 31;
@@ -595,8 +639,8 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
         }
         __syncwarp(gmask);
         if (rlo < D)
-            build_rows_flat<G>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb[gid], s_pre[gid], (uint32_t)glane, (uint32_t)G,
-                               gmask, [&](uint32_t i, uint32_t k) {
+            build_rows_flat<G>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb[gid], s_pre[gid], s_len[gid], (uint32_t)glane,
+                               (uint32_t)G, gmask, [&](uint32_t i, uint32_t k) {
                                    if (i >= rlo)
                                        atomicOr((unsigned long long *)&rows[i - rlo], 1ull << k);
                                    if (k >= rlo)
@@ -636,7 +680,8 @@ __global__ void __launch_bounds__(1024) k_medium(const PairDev *__restrict__ pai
     uint32_t *A = sm;
     uint32_t *s_hb = sm + pad;
     uint32_t *s_pre = sm + 2 * pad;
-    uint32_t *rows = sm + 3 * pad;
+    uint32_t *s_len = sm + 3 * pad;
+    uint32_t *rows = sm + 4 * pad;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
     EnumCtx ec;
@@ -672,7 +717,7 @@ __global__ void __launch_bounds__(1024) k_medium(const PairDev *__restrict__ pai
             s_j = j0;
         __syncthreads();
         if (rlo < D) // block-uniform
-            build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, threadIdx.x, blockDim.x, kFull,
+            build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, s_len, threadIdx.x, blockDim.x, kFull,
                                [&](uint32_t i, uint32_t k) {
                                    if (i >= rlo)
                                        atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
@@ -735,7 +780,7 @@ __global__ void __launch_bounds__(512) k_large_rows(const PairDev *__restrict__ 
                                                     unsigned *cursor) {
     extern __shared__ __align__(16) uint32_t sA[];
     __shared__ uint32_t s_c;
-    __shared__ uint32_t s_hb[kRowsPerChunk], s_pre[kRowsPerChunk + 1];
+    __shared__ uint32_t s_hb[kRowsPerChunk], s_len[kRowsPerChunk], s_pre[kRowsPerChunk + 1];
     const uint32_t total = bt.cstart[bt.nb];
     for (;;) {
         if (threadIdx.x == 0)
@@ -763,7 +808,7 @@ __global__ void __launch_bounds__(512) k_large_rows(const PairDev *__restrict__ 
             A = sA;
         }
         if (rlo < D) // block-uniform
-            build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, i0, i1, s_hb, s_pre, threadIdx.x, blockDim.x, kFull,
+            build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, i0, i1, s_hb, s_pre, s_len, threadIdx.x, blockDim.x, kFull,
                                [&](uint32_t i, uint32_t k) {
                                    if (i >= rlo)
                                        atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
@@ -1396,7 +1441,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         const uint32_t maxD = tier_max[k];
         const uint32_t W = (maxD + 31) / 32;
         const size_t pad = (maxD + 4) & ~3u;
-        const size_t smem = (3 * pad + (size_t)maxD * W) * 4;
+        const size_t smem = (4 * pad + (size_t)maxD * W) * 4;
         const int block = sub == 0 ? 256 : 1024;
         const int per_sm = std::max(1, (int)std::min<size_t>(2048 / block, (200 * 1024) / (smem + 1024)));
         uint32_t first = 0;

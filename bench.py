@@ -544,6 +544,18 @@ def main():
     e_ms = max_over_ranks(e_ms, world)
     e2e_value = world * (e_total // args.steps) / (e_ms / args.steps / 1e3)
 
+    # host->device copy of one step's inputs alone (pinned buffers, same stream), to explain e2e - value
+    with torch.cuda.stream(stream):
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(3):
+            d_rp.copy_(h_rp, non_blocking=True)
+            d_col.copy_(h_col, non_blocking=True)
+        c1.record(stream)
+    c1.synchronize()
+    h2d_ms = c0.elapsed_time(c1) / 3
+
     # wall-clock of each public call in one untimed step (the calls return after their device work)
     host_ms = {}
     torch.cuda.synchronize()
@@ -593,7 +605,8 @@ def main():
                    "matches_per_step": per_step, "l2": "flushed (256 MB write) before every step",
                    "step": "device CSR build + per-pattern peel/relabel + count"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * (n + 1) + 4 * m),
-                "d2h_bytes_per_step": 8 * len(queries) + 16, "ms_per_step": e_ms / args.steps},
+                "d2h_bytes_per_step": 8 * len(queries) + 16, "ms_per_step": e_ms / args.steps,
+                "h2d_copy_ms": h2d_ms},
         "gpu_launches": int(launches),
         "host_calls_ms": host_ms,
         "phases_ms_per_step": {"prep": prep_ms / args.steps, "count": count_ms / args.steps,
