@@ -253,19 +253,22 @@ __global__ void k_peel_chunks(const uint32_t *__restrict__ col, const uint8_t *_
 // Priority key (subgraph_matching.cuh:1299-1331, host_utils.cuh:230-246):
 // ascending (degree, id) or descending degree with ties by ascending id.
 // Vertices left with no edge get the largest key and are dropped.
+// The key is the degree part alone; a stable radix sort of (key, id) pairs
+// with ids in increasing order keeps ties by ascending id.
 __global__ void k_prio_keys(const uint32_t *__restrict__ deg, int64_t n, uint32_t maxdeg, int asc,
-                            uint64_t *keys, unsigned long long *n_alive) {
+                            uint32_t *keys, uint32_t *ids, unsigned long long *n_alive) {
     unsigned long long c = 0;
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t d = deg[v];
-        uint64_t hi;
+        uint32_t k;
         if (d == 0) {
-            hi = maxdeg;
+            k = maxdeg;
         } else {
-            hi = asc ? (uint64_t)(d - 1) : (uint64_t)(maxdeg - d);
+            k = asc ? d - 1 : maxdeg - d;
             ++c;
         }
-        keys[v] = (hi << 32) | (uint64_t)v;
+        keys[v] = k;
+        ids[v] = (uint32_t)v;
     }
     for (int o = 16; o > 0; o >>= 1)
         c += __shfl_xor_sync(kFull, c, o);
@@ -277,12 +280,12 @@ __global__ void k_prio_keys(const uint32_t *__restrict__ deg, int64_t n, uint32_
 // are listed here for a segmented sort.
 constexpr uint32_t kSortShort = 32;
 
-__global__ void k_rank(const uint64_t *__restrict__ keys, int64_t n_alive, uint32_t *orig, uint32_t *rank,
+__global__ void k_rank(const uint32_t *__restrict__ sorted_ids, int64_t n_alive, uint32_t *orig, uint32_t *rank,
                        const uint32_t *__restrict__ deg, uint32_t *new_deg, uint32_t *long_rows,
                        unsigned *n_long) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_alive;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t v = (uint32_t)keys[i];
+        const uint32_t v = sorted_ids[i];
         const uint32_t d = deg[v];
         orig[i] = v;
         rank[v] = (uint32_t)i;
@@ -641,7 +644,8 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     const uint32_t *col = g->col.as<uint32_t>();
     const int64_t nn = n > 0 ? n : 1;
     const size_t cap = chunk_capacity(n, m);
-    size_t need = Carve::need({(size_t)nn * 4, (size_t)nn, (size_t)nn * 4, (size_t)nn * 8, (size_t)nn * 8,
+    size_t need = Carve::need({(size_t)nn * 4, (size_t)nn, (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4,
+                               (size_t)nn * 4, (size_t)nn * 4,
                                (size_t)nn * 4, (size_t)(m > 0 ? m : 1) * 4, cap * sizeof(RowChunk), 16,
                                (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4});
     BEEP_TRY(ctx->grow(ctx->scratch2, need));
@@ -649,8 +653,8 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     uint32_t *deg = cv.take<uint32_t>(nn);
     uint8_t *alive = cv.take<uint8_t>(nn);
     uint32_t *rank = cv.take<uint32_t>(nn);
-    uint64_t *keys = cv.take<uint64_t>(nn);
-    uint64_t *keys2 = cv.take<uint64_t>(nn);
+    uint32_t *pkey = cv.take<uint32_t>(nn), *pid = cv.take<uint32_t>(nn);
+    uint32_t *pkey2 = cv.take<uint32_t>(nn), *pid2 = cv.take<uint32_t>(nn);
     uint32_t *new_deg = cv.take<uint32_t>(nn);
     uint32_t *col_tmp = cv.take<uint32_t>(m > 0 ? m : 1);
     RowChunk *chunks = cv.take<RowChunk>(cap);
@@ -705,14 +709,14 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     unsigned long long *d_alive = d_removed + 1;
     BEEP_CUDA_TRY(cudaMemsetAsync(d_alive, 0, 8, s));
     if (n > 0) {
-        k_prio_keys<<<gv, 256, 0, s>>>(deg, n, maxdeg, asc, keys, d_alive);
+        k_prio_keys<<<gv, 256, 0, s>>>(deg, n, maxdeg, asc, pkey, pid, d_alive);
         ++ctx->launches;
     }
     BEEP_CUDA_TRY(cudaGetLastError());
     size_t tb = 0;
-    BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys, keys2, n, 0, 32 + hb, s));
+    BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, pkey, pkey2, pid, pid2, n, 0, hb, s));
     BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
-    BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(ctx->scratch.ptr, tb, keys, keys2, n, 0, 32 + hb, s));
+    BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ctx->scratch.ptr, tb, pkey, pkey2, pid, pid2, n, 0, hb, s));
     // number of vertices that kept an edge
     BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, d_alive, 8, cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
@@ -726,7 +730,7 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_CUDA_TRY(cudaMemsetAsync(new_deg, 0, (size_t)nn * 4, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks + 1, 0, 4, s));
     if (na > 0) {
-        k_rank<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(keys2, na, v->orig.as<uint32_t>(), rank, deg,
+        k_rank<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(pid2, na, v->orig.as<uint32_t>(), rank, deg,
                                                                new_deg, long_rows, d_nchunks + 1);
         ++ctx->launches;
     }
