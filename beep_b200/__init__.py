@@ -177,6 +177,7 @@ _SIGNATURES = [
                                          _P(ctypes.c_int64), _P(ctypes.c_int64), _P(ctypes.c_int32),
                                          _P(ctypes.c_int32)]),
     ("beep_write_bel", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_int32)]),
+    ("beep_convert", ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, _P(ctypes.c_uint64)]),
 ]
 
 
@@ -609,3 +610,18 @@ class SG_Match:
         if verbose:
             print(f"------------- Counter = {c}")
         return c
+
+
+# the reference's -m converter tasks (src/main.cu:40-67)
+CONVERT_TASKS = {"txt-bel": 0, "mtx-bel": 1, "tsv-bel": 2, "tsv-mtx": 3, "bel-mtx": 4}
+
+
+def convert(task: str, src_path: str, dst_path: str) -> int:
+    """Convert a graph file as the reference's `-m <task> -g src -r dst` does
+    (graph::MtB_Writer, include/FIleReader.cuh:456-912). Returns the records
+    (or Matrix Market entries) written."""
+    if task not in CONVERT_TASKS:
+        raise BeepError(ERR_INVALID_ARG, f"unknown converter task {task!r}")
+    n = ctypes.c_uint64(0)
+    _check(lib().beep_convert(CONVERT_TASKS[task], os.fsencode(src_path), os.fsencode(dst_path), ctypes.byref(n)))
+    return int(n.value)

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", HOST_CXX, "-I", INCLUDE,
           "-Xcompiler", "-fPIC,-fopenmp,-Wall", "-Wno-deprecated-declarations"]
 
-LIB_SOURCES = ["graph.cu", "count.cu", "plan.cpp", "io.cpp", "api.cpp", "serve.cpp"]
+LIB_SOURCES = ["graph.cu", "count.cu", "plan.cpp", "io.cpp", "convert.cpp", "api.cpp", "serve.cpp"]
 HEADERS = ["internal.h"]
 
 

@@ -2,7 +2,10 @@
 // (src/main.cu:27-344, flags from include/Config.h:336-429):
 //   beep -g <data.bel> -t <query.mtx> -m sgm|sgc [-d <device>]
 // prints the reference's result line "------------- Counter = N"
-// (subgraph_matching/subgraph_matching.cuh:1277) and its timing lines.
+// (subgraph_matching/subgraph_matching.cuh:1277) and its timing lines;
+//   beep -m txt-bel|mtx-bel|tsv-bel|tsv-mtx|bel-mtx -g <src> -r <dst>
+// converts a graph file as the reference does (src/main.cu:40-67). The
+// converters need no GPU.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -18,9 +21,11 @@ namespace {
 void usage(const char *argv0) {
     std::printf("Usage:  %s [options]\n\n"
                 "Options:\n"
-                "    -g <Src graph FileName>       data graph (.bel)\n"
+                "    -g <Src graph FileName>       data graph (.bel); the input file of a conversion\n"
+                "    -r <Dst graph FileName>       the output file of a conversion\n"
                 "    -t <Pattern graph filename>   query graph (.mtx, 0-based, both directions)\n"
-                "    -m <MainTask>                 sgm (enumeration count) or sgc (counting)\n"
+                "    -m <MainTask>                 sgm (enumeration count) or sgc (counting), or a converter:\n"
+                "                                  txt-bel, mtx-bel, tsv-bel, tsv-mtx, bel-mtx\n"
                 "    -d <Device Id>                GPU device id (default = 0)\n"
                 "    -s                            accepted for compatibility (edges are always sorted)\n"
                 "    -c <cutoff>                   accepted for compatibility (recomputed from the degrees)\n"
@@ -38,13 +43,16 @@ int die(const char *what, beep_status s) {
 } // namespace
 
 int main(int argc, char **argv) {
-    const char *gpath = nullptr, *tpath = nullptr, *mode_s = "sgm";
+    const char *gpath = nullptr, *tpath = nullptr, *rpath = nullptr, *mode_s = "sgm";
     int dev = 0;
     int opt;
-    while ((opt = getopt(argc, argv, "g:t:m:d:sc:n:h")) != -1) {
+    while ((opt = getopt(argc, argv, "g:r:t:m:d:sc:n:h")) != -1) {
         switch (opt) {
         case 'g':
             gpath = optarg;
+            break;
+        case 'r':
+            rpath = optarg;
             break;
         case 't':
             tpath = optarg;
@@ -70,6 +78,27 @@ int main(int argc, char **argv) {
             return opt == 'h' ? 0 : 1;
         }
     }
+    static const struct {
+        const char *name;
+        beep_convert_task task;
+    } convs[] = {{"txt-bel", BEEP_CONV_TXT_BEL},
+                 {"mtx-bel", BEEP_CONV_MTX_BEL},
+                 {"tsv-bel", BEEP_CONV_TSV_BEL},
+                 {"tsv-mtx", BEEP_CONV_TSV_MTX},
+                 {"bel-mtx", BEEP_CONV_BEL_MTX}};
+    for (const auto &c : convs)
+        if (std::strcmp(mode_s, c.name) == 0) {
+            if (!gpath || !rpath) {
+                usage(argv[0]);
+                return 1;
+            }
+            uint64_t written = 0;
+            beep_status s = beep_convert(c.task, gpath, rpath, &written);
+            if (s)
+                return die(c.name, s);
+            std::printf("%s: %llu records written to %s\n", c.name, (unsigned long long)written, rpath);
+            return 0;
+        }
     beep_mode mode;
     if (std::strcmp(mode_s, "sgm") == 0)
         mode = BEEP_MODE_SGM;

@@ -276,143 +276,69 @@ __global__ void k_prio_keys(const uint32_t *__restrict__ deg, int64_t n, uint32_
         atomicAdd(n_alive, c);
 }
 
-// Rows of at most kSortShort entries are sorted by k_sort_short; longer ones
-// are listed here for a segmented sort.
-constexpr uint32_t kSortShort = 32;
-
 __global__ void k_rank(const uint32_t *__restrict__ sorted_ids, int64_t n_alive, uint32_t *orig, uint32_t *rank,
-                       const uint32_t *__restrict__ deg, uint32_t *new_deg, uint32_t *long_rows,
-                       unsigned *n_long) {
+                       const uint32_t *__restrict__ deg, uint32_t *new_deg) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_alive;
          i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t v = sorted_ids[i];
-        const uint32_t d = deg[v];
         orig[i] = v;
         rank[v] = (uint32_t)i;
-        new_deg[i] = d;
-        if (d > kSortShort)
-            long_rows[atomicAdd(n_long, 1u)] = (uint32_t)i;
+        new_deg[i] = deg[v];
     }
 }
 
-__global__ void k_long_offsets(const uint32_t *__restrict__ long_rows, const unsigned *__restrict__ n_long,
-                               const uint32_t *__restrict__ rp, uint32_t *beg, uint32_t *end) {
-    const uint32_t nl = *n_long;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nl; k += gridDim.x * blockDim.x) {
-        const uint32_t i = long_rows[k];
-        beg[k] = rp[i];
-        end[k] = rp[i + 1];
-    }
+// The relabelled rows are produced by one sort: every input entry (v, w)
+// becomes the key (rank v) << rb | rank w (ranks < 2^rb), or ~0 when either
+// end was dropped,
+// written at the entry's own position; sorting the keys leaves the new rows
+// in order, each sorted, with the dropped entries after them. No per-row
+// sort, so a few very long rows (hubs) cannot hold up the rest.
+__device__ __forceinline__ uint64_t view_key(uint32_t rv, uint32_t rw, int rb) {
+    return (rv == 0xffffffffu || rw == 0xffffffffu) ? ~0ull : (((uint64_t)rv << rb) | rw);
 }
 
-// Ascending bitonic sort of one value per lane across a group of G lanes.
-template <int G> __device__ __forceinline__ uint32_t bitonic_sort(uint32_t x, int glane) {
-#pragma unroll
-    for (int k = 2; k <= G; k <<= 1)
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            const uint32_t y = __shfl_xor_sync(kFull, x, j, G);
-            x = (((glane & j) == 0) == ((glane & k) == 0)) ? min(x, y) : max(x, y);
-        }
-    return x;
-}
-
-// Sorts the rows of at most kSortShort entries from `in` into `out` (same
-// offsets). A warp takes four rows: when all four have at most 8 entries each
-// 8-lane group sorts one, otherwise the warp sorts them one after the other.
-__global__ void k_sort_short(const uint32_t *__restrict__ rp, int64_t n, const uint32_t *__restrict__ in,
-                             uint32_t *out) {
+__global__ void k_fill_keys(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
+                            const uint32_t *__restrict__ rank, int64_t n, int rb, uint64_t *keys,
+                            RowChunk *chunks, unsigned *n_chunks, uint32_t cap) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; base < n; base += warps * 4) {
-        const int64_t my = base + (lane >> 3);
-        uint32_t b = 0, L = 0;
-        if (my < n) {
-            b = rp[my];
-            L = rp[my + 1] - b;
-        }
-        if (__all_sync(kFull, L <= 8)) {
-            const int g = lane & 7;
-            uint32_t x = (uint32_t)g < L ? in[b + g] : 0xffffffffu;
-            x = bitonic_sort<8>(x, g);
-            if ((uint32_t)g < L)
-                out[b + g] = x;
-        } else {
-            for (int r = 0; r < 4; ++r) {
-                const uint32_t rb = __shfl_sync(kFull, b, r * 8), rl = __shfl_sync(kFull, L, r * 8);
-                if (rl > kSortShort) // warp-uniform
-                    continue;
-                uint32_t x = (uint32_t)lane < rl ? in[rb + lane] : 0xffffffffu;
-                x = bitonic_sort<32>(x, lane);
-                if ((uint32_t)lane < rl)
-                    out[rb + lane] = x;
-            }
-        }
-    }
-}
-
-// Row i of the relabelled graph: ranks of the surviving neighbours of
-// orig[i], in any order (the rows are sorted afterwards). Short rows keep
-// input order; the chunks of long rows take their places in the row through
-// a per-row cursor (cursor[i], zeroed here).
-__global__ void k_fill_rows(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
-                            const uint32_t *__restrict__ orig, const uint32_t *__restrict__ rank,
-                            const uint32_t *__restrict__ new_rp, int64_t n_alive, uint32_t *new_col,
-                            uint32_t *cursor, RowChunk *chunks, unsigned *n_chunks, uint32_t cap) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n_alive;
-         base += warps * 32) {
-        const int64_t i = base + lane;
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += warps * 32) {
+        const int64_t v = base + lane;
         bool big = false;
         uint32_t b = 0, e = 0;
-        if (i < n_alive) {
-            const uint32_t v = orig[i];
+        if (v < n) {
             b = rp[v];
             e = rp[v + 1];
             if (e - b > kSerialMax) {
                 big = true;
-                cursor[i] = 0;
             } else {
-                uint32_t out = new_rp[i];
-                for (uint32_t k = b; k < e; ++k) {
-                    const uint32_t r = rank[col[k]];
-                    if (r != 0xffffffffu)
-                        new_col[out++] = r;
-                }
+                const uint32_t rv = rank[v];
+                for (uint32_t k = b; k < e; ++k)
+                    keys[k] = view_key(rv, rank[col[k]], rb);
             }
         }
-        push_chunks(big, (uint32_t)i, b, e, chunks, n_chunks, cap, lane);
+        push_chunks(big, (uint32_t)v, b, e, chunks, n_chunks, cap, lane);
     }
 }
 
-__global__ void k_fill_chunks(const uint32_t *__restrict__ col, const uint32_t *__restrict__ rank,
-                              const uint32_t *__restrict__ new_rp, const RowChunk *__restrict__ chunks,
-                              const unsigned *__restrict__ n_chunks, uint32_t cap, uint32_t *cursor,
-                              uint32_t *new_col) {
+__global__ void k_fill_key_chunks(const uint32_t *__restrict__ col, const uint32_t *__restrict__ rank,
+                                  const RowChunk *__restrict__ chunks, const unsigned *__restrict__ n_chunks,
+                                  uint32_t cap, int rb, uint64_t *keys) {
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t nc = min(*n_chunks, cap);
     for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc; c += warps) {
         const RowChunk ch = chunks[c];
-        const uint32_t row_base = new_rp[ch.row];
-        for (uint32_t k0 = ch.b; k0 < ch.e; k0 += 32) {
-            const uint32_t k = k0 + lane;
-            uint32_t r = 0xffffffffu;
-            if (k < ch.e)
-                r = rank[col[k]];
-            const bool keep = r != 0xffffffffu;
-            const unsigned bal = __ballot_sync(kFull, keep);
-            if (!bal)
-                continue;
-            uint32_t at = 0;
-            if (lane == 0)
-                at = atomicAdd(&cursor[ch.row], (uint32_t)__popc(bal));
-            at = __shfl_sync(kFull, at, 0);
-            if (keep)
-                new_col[row_base + at + __popc(bal & ((1u << lane) - 1u))] = r;
-        }
+        const uint32_t rv = rank[ch.row];
+        for (uint32_t k = ch.b + lane; k < ch.e; k += 32)
+            keys[k] = view_key(rv, rank[col[k]], rb);
     }
+}
+
+__global__ void k_keys_low(const uint64_t *__restrict__ keys, int64_t m, int rb, uint32_t *col) {
+    const uint64_t mask = ((uint64_t)1 << rb) - 1;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        col[i] = (uint32_t)(keys[i] & mask);
 }
 
 // split[i] = number of neighbours with a smaller new id (lower_bound of i).
@@ -644,10 +570,10 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     const uint32_t *col = g->col.as<uint32_t>();
     const int64_t nn = n > 0 ? n : 1;
     const size_t cap = chunk_capacity(n, m);
+    const size_t mm = m > 0 ? (size_t)m : 1;
     size_t need = Carve::need({(size_t)nn * 4, (size_t)nn, (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4,
-                               (size_t)nn * 4, (size_t)nn * 4,
-                               (size_t)nn * 4, (size_t)(m > 0 ? m : 1) * 4, cap * sizeof(RowChunk), 16,
-                               (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4});
+                               (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4, mm * 8, mm * 8,
+                               cap * sizeof(RowChunk), 16});
     BEEP_TRY(ctx->grow(ctx->scratch2, need));
     Carve cv(ctx->scratch2.ptr);
     uint32_t *deg = cv.take<uint32_t>(nn);
@@ -656,12 +582,9 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     uint32_t *pkey = cv.take<uint32_t>(nn), *pid = cv.take<uint32_t>(nn);
     uint32_t *pkey2 = cv.take<uint32_t>(nn), *pid2 = cv.take<uint32_t>(nn);
     uint32_t *new_deg = cv.take<uint32_t>(nn);
-    uint32_t *col_tmp = cv.take<uint32_t>(m > 0 ? m : 1);
+    uint64_t *ekeys = cv.take<uint64_t>(mm), *ekeys2 = cv.take<uint64_t>(mm);
     RowChunk *chunks = cv.take<RowChunk>(cap);
-    unsigned *d_nchunks = cv.take<unsigned>(4); // [0] chunks, [1] long rows
-    uint32_t *long_rows = cv.take<uint32_t>(nn);
-    uint32_t *long_beg = cv.take<uint32_t>(nn);
-    uint32_t *long_end = cv.take<uint32_t>(nn);
+    unsigned *d_nchunks = cv.take<unsigned>(4);
     const uint32_t ucap = (uint32_t)std::min<size_t>(cap, 0xffffffffu);
     BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned long long *d_removed = ctx->counter.as<unsigned long long>();
@@ -728,10 +651,9 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_TRY(ctx->grow(v->split, (size_t)(na > 0 ? na : 1) * 4));
     BEEP_CUDA_TRY(cudaMemsetAsync(rank, 0xff, (size_t)nn * 4, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(new_deg, 0, (size_t)nn * 4, s));
-    BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks + 1, 0, 4, s));
     if (na > 0) {
         k_rank<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(pid2, na, v->orig.as<uint32_t>(), rank, deg,
-                                                               new_deg, long_rows, d_nchunks + 1);
+                                                               new_deg);
         ++ctx->launches;
     }
     BEEP_CUDA_TRY(cudaGetLastError());
@@ -742,41 +664,31 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ctx->scratch.ptr, tb, new_deg, nrp, na + 1, s));
     uint32_t *h2 = reinterpret_cast<uint32_t *>(ctx->h_pinned);
     BEEP_CUDA_TRY(cudaMemcpyAsync(h2, nrp + na, 4, cudaMemcpyDeviceToHost, s));
-    BEEP_CUDA_TRY(cudaMemcpyAsync(h2 + 1, d_nchunks + 1, 4, cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
-    const uint32_t h_m = h2[0], n_long = h2[1];
+    const uint32_t h_m = h2[0];
     v->m = h_m;
     tr.mark("rank_scan");
     BEEP_TRY(ctx->grow(v->col, (size_t)(h_m > 0 ? h_m : 1) * 4));
-    if (na > 0) {
+    // rank bits: every rank is below na < 2^rb
+    int rb = 1;
+    while (rb < 32 && ((uint64_t)1 << rb) <= (uint64_t)na)
+        ++rb;
+    if (h_m > 0) {
         BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks, 0, 4, s));
-        k_fill_rows<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(rp, col, v->orig.as<uint32_t>(), rank,
-                                                                           nrp, na, col_tmp, new_deg, chunks,
-                                                                           d_nchunks, ucap);
-        k_fill_chunks<<<ctx->num_sms * 8, 256, 0, s>>>(col, rank, nrp, chunks, d_nchunks, ucap, new_deg, col_tmp);
+        k_fill_keys<<<gv, 256, 0, s>>>(rp, col, rank, n, rb, ekeys, chunks, d_nchunks, ucap);
+        k_fill_key_chunks<<<ctx->num_sms * 8, 256, 0, s>>>(col, rank, chunks, d_nchunks, ucap, rb, ekeys);
         ctx->launches += 2;
+        BEEP_CUDA_TRY(cudaGetLastError());
     }
-    BEEP_CUDA_TRY(cudaGetLastError());
     tr.mark("fill");
-    // Sort every row: short rows by warps, the long ones by a segmented sort
-    // over their segments only (CUB leaves keys outside the segments alone).
-    if (na > 0 && h_m > 0) {
-        k_sort_short<<<grid_for((na + 3) / 4 * 32, 256, ctx->num_sms), 256, 0, s>>>(nrp, na, col_tmp,
-                                                                                 v->col.as<uint32_t>());
-        ++ctx->launches;
-        BEEP_CUDA_TRY(cudaGetLastError());
-    }
-    if (n_long > 0) {
-        k_long_offsets<<<grid_for(n_long, 256, ctx->num_sms), 256, 0, s>>>(long_rows, d_nchunks + 1, nrp,
-                                                                           long_beg, long_end);
-        ++ctx->launches;
-        BEEP_CUDA_TRY(cudaGetLastError());
+    if (h_m > 0) {
         tb = 0;
-        BEEP_CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(nullptr, tb, col_tmp, v->col.as<uint32_t>(), (int64_t)h_m,
-                                                         (int64_t)n_long, long_beg, long_end, s));
+        BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, ekeys, ekeys2, m, 0, 2 * rb, s));
         BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
-        BEEP_CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(ctx->scratch.ptr, tb, col_tmp, v->col.as<uint32_t>(),
-                                                         (int64_t)h_m, (int64_t)n_long, long_beg, long_end, s));
+        BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(ctx->scratch.ptr, tb, ekeys, ekeys2, m, 0, 2 * rb, s));
+        k_keys_low<<<grid_for(h_m, 256, ctx->num_sms), 256, 0, s>>>(ekeys2, h_m, rb, v->col.as<uint32_t>());
+        ++ctx->launches;
+        BEEP_CUDA_TRY(cudaGetLastError());
     }
     if (na > 0) {
         k_split<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(nrp, v->col.as<uint32_t>(), na,

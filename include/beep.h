@@ -321,6 +321,22 @@ beep_status beep_gen_chung_lu(int64_t n, double avg_degree, double exponent, uin
  * read_bel consumes (include/FIleReader.cuh:63-89). */
 beep_status beep_write_bel(const char *path, int64_t n, const int32_t *row_ptr, const int32_t *col_ind);
 
+/* ---- file converters (the reference's -m txt-bel | mtx-bel | tsv-bel |
+ * tsv-mtx | bel-mtx, src/main.cu:40-67 over graph::MtB_Writer,
+ * include/FIleReader.cuh:456-912) ----------------------------------------- */
+typedef enum beep_convert_task {
+    BEEP_CONV_TXT_BEL = 0, /* "a b" lines, '%' comments -> both directions, sorted, unique */
+    BEEP_CONV_MTX_BEL = 1, /* Matrix Market -> sorted records, mirrored when symmetric */
+    BEEP_CONV_TSV_BEL = 2, /* "dst src weight" triples -> records in file order */
+    BEEP_CONV_TSV_MTX = 3, /* "dst src weight" triples -> Matrix Market */
+    BEEP_CONV_BEL_MTX = 4  /* .bel records -> Matrix Market */
+} beep_convert_task;
+/* Converts src_path into dst_path with the bytes the reference's converter
+ * writes; *records_out (may be NULL) receives the records or entries written.
+ * Inputs the reference cannot finish (no edges for a Matrix Market output, a
+ * missing size line) return BEEP_ERR_PARSE instead. */
+beep_status beep_convert(beep_convert_task task, const char *src_path, const char *dst_path, uint64_t *records_out);
+
 #ifdef __cplusplus
 }
 #endif
