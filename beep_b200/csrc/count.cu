@@ -228,46 +228,94 @@ __device__ __forceinline__ void emit_bits(const EnumCtx &ec, const uint32_t (&x)
 // ---------------------------------------------------------------------------
 // thread-level DFS on 64-bit rows (D <= 64)
 // ---------------------------------------------------------------------------
-// rows[i - rlo] is the row of domain vertex i (only rows i >= rlo exist; the
-// plan reads no other).
-template <int P, int DEND, bool ENUM>
-__device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, uint32_t rlo, uint64_t all,
-                                           uint32_t (&x)[kMaxQ], unsigned long long &cnt, const EnumCtx &ec) {
-    bool closed = false; // count this level's candidates as C(A, DEND - P)
-    if constexpr (!ENUM && DEND - P <= 4) {
-        const uint32_t lo = level_bound<P>(lp, x);
-        if (suffix_applies<P, DEND>(lp, x, lo)) {
-            if (lp.free_back == 0) {
-                cnt += binom_le4(free_count_rootonly<P>((uint32_t)__popcll(all), x, lo), DEND - P);
-                return;
-            }
-            closed = true;
-        }
-    }
-    uint64_t c = all;
-    const uint32_t bk = lp.back[P], sy = lp.sym[P];
+// rows + (i - rlo) * NW is the row of domain vertex i, NW 64-bit words (only
+// rows i >= rlo exist; the plan reads no other). One thread walks the whole
+// subtree below its level-1 vertex; the candidate words of a level stay in
+// registers.
+// Word k of position P's candidate set: the domain bits at or above lo, AND
+// the rows of P's back edges, minus the vertices already used.
+template <int P, int NW>
+__device__ __forceinline__ uint64_t cand_word(const Lp &lp, const uint64_t *rows, uint32_t rlo, uint32_t D,
+                                              uint32_t lo, const uint32_t (&x)[kMaxQ], uint32_t k) {
+    const uint32_t base = k * 64;
+    uint64_t w = base + 64 <= D ? ~0ull : (base < D ? ((1ull << (D - base)) - 1ull) : 0ull);
+    if (lo > base)
+        w = lo >= base + 64 ? 0ull : (w & ~((1ull << (lo - base)) - 1ull));
+    const uint32_t bk = lp.back[P];
 #pragma unroll
     for (int q = 1; q < P; ++q) {
         if (bk >> q & 1u)
-            c &= rows[x[q] - rlo];
-        c &= ~(1ull << x[q]);
-        if (sy >> q & 1u)
-            c &= ~((2ull << x[q]) - 1ull); // keep bits above x[q]
+            w &= rows[(size_t)(x[q] - rlo) * NW + k];
+        if ((x[q] >> 6) == k)
+            w &= ~(1ull << (x[q] & 63));
     }
-    if (closed) {
-        cnt += binom_le4((uint32_t)__popcll(c), DEND - P);
+    return w;
+}
+
+template <int P, int DEND, bool ENUM, int NW>
+__device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, uint32_t rlo, uint32_t D,
+                                           uint32_t (&x)[kMaxQ], unsigned long long &cnt, const EnumCtx &ec) {
+    const uint32_t lo = level_bound<P>(lp, x);
+    bool closed = false; // count this level's candidates as C(A, DEND - P)
+    if constexpr (!ENUM && DEND - P <= 4) {
+        if (suffix_applies<P, DEND>(lp, x, lo)) {
+            if (lp.free_back == 0) {
+                cnt += binom_le4(free_count_rootonly<P>(D, x, lo), DEND - P);
+                return;
+            }
+            closed = DEND - P >= 2; // one level: the leaf popcount below is the same
+        }
+    }
+    if constexpr (NW == 1) {
+        // one word: the candidate set stays in a register
+        uint64_t c = cand_word<P, 1>(lp, rows, rlo, D, lo, x, 0);
+        if (closed) {
+            cnt += binom_le4((uint32_t)__popcll(c), DEND - P);
+            return;
+        }
+        if constexpr (P == DEND - 1) {
+            if constexpr (ENUM)
+                emit_bits(ec, x, P, c, 0);
+            cnt += (unsigned long long)__popcll(c);
+        } else {
+            while (c) {
+                const int b = __ffsll((long long)c) - 1;
+                c &= c - 1;
+                x[P] = (uint32_t)b;
+                dfs_thread<P + 1, DEND, ENUM, 1>(lp, rows, rlo, D, x, cnt, ec);
+            }
+        }
         return;
     }
-    if constexpr (P == DEND - 1) {
-        if constexpr (ENUM)
-            emit_bits(ec, x, P, c, 0);
-        cnt += (unsigned long long)__popcll(c);
-    } else {
-        while (c) {
-            const int b = __ffsll((long long)c) - 1;
-            c &= c - 1;
-            x[P] = (uint32_t)b;
-            dfs_thread<P + 1, DEND, ENUM>(lp, rows, rlo, all, x, cnt, ec);
+    const uint32_t k0 = lo >> 6, nw = min((uint32_t)NW, (D + 63) >> 6);
+    if (closed || P == DEND - 1) {
+        uint32_t A = 0;
+        for (uint32_t k = k0; k < nw; ++k) {
+            const uint64_t w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
+            if constexpr (ENUM)
+                emit_bits(ec, x, P, w, k * 64);
+            A += (uint32_t)__popcll(w);
+        }
+        cnt += closed ? binom_le4(A, DEND - P) : (unsigned long long)A;
+        return;
+    }
+    if constexpr (P < DEND - 1 && NW > 1) {
+        // one call site per level; only the current word and its index live
+        // across the call (the next word is recomputed from the rows)
+        uint32_t k = k0;
+        if (k >= nw)
+            return;
+        uint64_t w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
+        for (;;) {
+            while (!w) {
+                if (++k >= nw)
+                    return;
+                w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
+            }
+            const int b = __ffsll((long long)w) - 1;
+            w &= w - 1;
+            x[P] = k * 64 + (uint32_t)b;
+            dfs_thread<P + 1, DEND, ENUM, NW>(lp, rows, rlo, D, x, cnt, ec);
         }
     }
 }
@@ -295,7 +343,7 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
                     cnt += binom_le4(free_count_rootonly<P>(D, x, lo), DEND - P);
                 return;
             }
-            closed = true;
+            closed = DEND - P >= 2; // one level: the leaf popcount below is the same
         }
     }
     const int gbase = (threadIdx.x & 31) & ~(G - 1);
@@ -647,7 +695,6 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
                                        atomicOr((unsigned long long *)&rows[k - rlo], 1ull << i);
                                });
         __syncwarp(gmask);
-        const uint64_t all = (D >= 64) ? ~0ull : ((1ull << D) - 1ull);
         if constexpr (ENUM) {
             ec.A = A;
             ec.root = r;
@@ -655,7 +702,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
         for (uint32_t j = j0 + glane; j < D; j += G) {
             uint32_t x[kMaxQ];
             x[1] = j;
-            dfs_thread<2, DEND, ENUM>(pr.lp, rows, rlo, all, x, cnt, ec);
+            dfs_thread<2, DEND, ENUM, 1>(pr.lp, rows, rlo, D, x, cnt, ec);
         }
         __syncwarp(gmask);
     }
@@ -667,10 +714,12 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
 // ---------------------------------------------------------------------------
 // medium tier: block per root, bitmap in shared memory
 // ---------------------------------------------------------------------------
-// G lanes per level-1 vertex: 8 for domains of at most 256 vertices (rows of
-// at most 8 words), 32 above.
+// G lanes per level-1 vertex (32: domains of up to 1024 vertices, rows of up
+// to 32 words walked a warp at a time), or G = 0: one thread per level-1
+// vertex over rows of 4 x 64 bits (domains of up to 256 vertices), the whole
+// subtree in registers.
 template <int DEND, bool ENUM, int G>
-__global__ void __launch_bounds__(1024) k_medium(const PairDev *__restrict__ pairs,
+__global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? 2 : 1) k_medium(const PairDev *__restrict__ pairs,
                                                 const uint64_t *__restrict__ items, uint32_t nitems,
                                                 unsigned *cursor, uint32_t maxD) {
     extern __shared__ __align__(16) uint32_t sm[];
@@ -709,38 +758,64 @@ __global__ void __launch_bounds__(1024) k_medium(const PairDev *__restrict__ pai
         pair_domain(pr, r, beg, D, j0);
         const uint32_t rlo = pair_rlo(pr, D, j0);
         const uint32_t W = (D + 31) >> 5;
+        constexpr uint32_t kThreadNW = 4;                  // 64-bit words per row in thread mode
+        const uint32_t row_words = G == 0 ? 2 * kThreadNW : W; // 32-bit words per row
         for (uint32_t i = threadIdx.x; i < D; i += blockDim.x)
             A[i] = pr.v.col[beg + i];
-        for (uint32_t i = threadIdx.x; i < (D - rlo) * W; i += blockDim.x)
+        for (uint32_t i = threadIdx.x; i < (D - rlo) * row_words; i += blockDim.x)
             rows[i] = 0;
         if (threadIdx.x == 0)
             s_j = j0;
         __syncthreads();
-        if (rlo < D) // block-uniform
-            build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, s_len, threadIdx.x, blockDim.x, kFull,
-                               [&](uint32_t i, uint32_t k) {
-                                   if (i >= rlo)
-                                       atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
-                                   if (k >= rlo)
-                                       atomicOr(&rows[(size_t)(k - rlo) * W + (i >> 5)], 1u << (i & 31));
-                               });
+        if (rlo < D) { // block-uniform
+            if constexpr (G == 0) {
+                unsigned long long *r64 = reinterpret_cast<unsigned long long *>(rows);
+                build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, s_len, threadIdx.x, blockDim.x,
+                                   kFull, [&](uint32_t i, uint32_t k) {
+                                       if (i >= rlo)
+                                           atomicOr(&r64[(size_t)(i - rlo) * kThreadNW + (k >> 6)], 1ull << (k & 63));
+                                       if (k >= rlo)
+                                           atomicOr(&r64[(size_t)(k - rlo) * kThreadNW + (i >> 6)], 1ull << (i & 63));
+                                   });
+            } else {
+                build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, s_len, threadIdx.x, blockDim.x,
+                                   kFull, [&](uint32_t i, uint32_t k) {
+                                       if (i >= rlo)
+                                           atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
+                                       if (k >= rlo)
+                                           atomicOr(&rows[(size_t)(k - rlo) * W + (i >> 5)], 1u << (i & 31));
+                                   });
+            }
+        }
         __syncthreads();
         if constexpr (ENUM) {
             ec.A = A;
             ec.root = r;
         }
-        const int glane = lane & (G - 1);
-        const unsigned gmask = G == 32 ? kFull : (((1u << G) - 1u) << (lane & ~(G - 1)));
-        for (;;) {
-            uint32_t j = 0;
-            if (glane == 0)
-                j = atomicAdd(&s_j, 1u);
-            j = __shfl_sync(gmask, j, 0, G);
-            if (j >= D)
-                break;
-            uint32_t x[kMaxQ];
-            x[1] = j;
-            dfs_warp<2, DEND, ENUM, G>(pr.lp, rows, rlo, W, D, x, cnt, glane, ec, gmask);
+        if constexpr (G == 0) {
+            const uint64_t *r64 = reinterpret_cast<const uint64_t *>(rows);
+            for (;;) {
+                const uint32_t j = atomicAdd(&s_j, 1u);
+                if (j >= D)
+                    break;
+                uint32_t x[kMaxQ];
+                x[1] = j;
+                dfs_thread<2, DEND, ENUM, kThreadNW>(pr.lp, r64, rlo, D, x, cnt, ec);
+            }
+        } else {
+            const int glane = lane & (G - 1);
+            const unsigned gmask = G == 32 ? kFull : (((1u << G) - 1u) << (lane & ~(G - 1)));
+            for (;;) {
+                uint32_t j = 0;
+                if (glane == 0)
+                    j = atomicAdd(&s_j, 1u);
+                j = __shfl_sync(gmask, j, 0, G);
+                if (j >= D)
+                    break;
+                uint32_t x[kMaxQ];
+                x[1] = j;
+                dfs_warp<2, DEND, ENUM, G>(pr.lp, rows, rlo, W, D, x, cnt, glane, ec, gmask);
+            }
         }
         __syncthreads();
     }
@@ -1033,7 +1108,7 @@ beep_status launch_small(int dend, int group, int grid, cudaStream_t s, const Pa
 }
 
 template <int D, bool ENUM> beep_status set_medium_attr(size_t smem) {
-    BEEP_CUDA_TRY(cudaFuncSetAttribute(k_medium<D, ENUM, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BEEP_CUDA_TRY(cudaFuncSetAttribute(k_medium<D, ENUM, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     BEEP_CUDA_TRY(cudaFuncSetAttribute(k_medium<D, ENUM, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     return BEEP_OK;
 }
@@ -1439,7 +1514,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         uint64_t *list = nullptr;
         BEEP_TRY(make_list(k, list));
         const uint32_t maxD = tier_max[k];
-        const uint32_t W = (maxD + 31) / 32;
+        // 32-bit words per row: 8 (4 x 64 bits) in the thread-mode sub-tier
+        const uint32_t W = sub == 0 ? 8u : (maxD + 31) / 32;
         const size_t pad = (maxD + 4) & ~3u;
         const size_t smem = (4 * pad + (size_t)maxD * W) * 4;
         const int block = sub == 0 ? 256 : 1024;
@@ -1452,7 +1528,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             LaunchRec r;
             r.kind = LaunchRec::kMedium;
             r.dend = d;
-            r.group = sub == 0 ? 8 : 32;
+            r.group = sub == 0 ? 0 : 32;
             r.grid = ctx->num_sms * per_sm;
             r.block = block;
             r.smem = smem;
@@ -1568,12 +1644,12 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::ve
         case LaunchRec::kMedium:
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
-        if (lp->enumerate && r.group == 8)                                                                         \
-            k_medium<D, true, 8><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);    \
+        if (lp->enumerate && r.group == 0)                                                                         \
+            k_medium<D, true, 0><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);    \
         else if (lp->enumerate)                                                                                    \
             k_medium<D, true, 32><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);   \
-        else if (r.group == 8)                                                                                     \
-            k_medium<D, false, 8><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);   \
+        else if (r.group == 0)                                                                                     \
+            k_medium<D, false, 0><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);   \
         else                                                                                                       \
             k_medium<D, false, 32><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);  \
         break;
