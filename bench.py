@@ -102,6 +102,11 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi's own start-up takes driver time: let it finish (first
+        # sample printed) before the timed region begins
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 5.0:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -262,7 +267,10 @@ def reference_arm(args, wl):
                 # one untimed run per pattern (process start, module load, graph file cache)
                 for name in wl["patterns"][: 1 if args.warmup > 0 else 0]:
                     run_reference_binary(binary, bel, mtxs[name], wl["mode"], args.reference_timeout)
+                t_start = time.time()
                 for _ in range(args.steps):
+                    if times and time.time() - t_start > args.reference_budget:
+                        break  # bounded: each step is two full process runs
                     tot_t, cs = 0.0, []
                     for name in wl["patterns"]:
                         c, t = run_reference_binary(binary, bel, mtxs[name], wl["mode"], args.reference_timeout)
@@ -273,12 +281,13 @@ def reference_arm(args, wl):
                 med = statistics.median(times)
                 value = sum(counts) / med
                 line.update({"value": value, "ms_per_step": med * 1e3, "counts": dict(zip(wl["patterns"], counts)),
+                             "steps_run": len(times),
                              "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                                               "sample": "the reference's own sgm/sgc (src/main.cu built for sm_100a "
                                                         "by oracle/refbuild.py) run on the B200, one host thread; "
                                                         "time per step = its Transfer + Preprocessing + final count "
                                                         "lines for each pattern (file parsing excluded); median of "
-                                                        f"{args.steps} steps"},
+                                                        f"{len(times)} steps"},
                              "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                                      "d2h_bytes_per_step": 0}})
                 print(json.dumps(line), flush=True)
@@ -441,13 +450,15 @@ def bench_served(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-port", action="store_true", help="reference arm: use the CPU port")
     ap.add_argument("--reference-timeout", type=float, default=300.0)
+    ap.add_argument("--reference-budget", type=float, default=150.0,
+                    help="reference arm: stop starting new steps after this many seconds")
     ap.add_argument("--c4-graphs", type=int, default=256)
     ap.add_argument("--c4-max-scale", type=float, default=18.0)
     ap.add_argument("--c4-max-degree", type=float, default=64.0)
