@@ -252,6 +252,21 @@ __device__ __forceinline__ uint64_t cand_word(const Lp &lp, const uint64_t *rows
     return w;
 }
 
+// Position of the j-th set bit (0-based) of w, which has more than j set bits.
+__device__ __forceinline__ uint32_t select64(uint64_t w, uint32_t j) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (int sh = 32; sh >= 1; sh >>= 1) {
+        const uint32_t c = (uint32_t)__popcll(w & ((1ull << sh) - 1ull));
+        if (j >= c) {
+            j -= c;
+            w >>= sh;
+            pos += (uint32_t)sh;
+        }
+    }
+    return pos;
+}
+
 template <int P, int DEND, bool ENUM, int NW>
 __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, uint32_t rlo, uint32_t D,
                                            uint32_t (&x)[kMaxQ], unsigned long long &cnt, const EnumCtx &ec) {
@@ -794,13 +809,57 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? 2 : 1) k_medium(
         }
         if constexpr (G == 0) {
             const uint64_t *r64 = reinterpret_cast<const uint64_t *>(rows);
-            for (;;) {
-                const uint32_t j = atomicAdd(&s_j, 1u);
-                if (j >= D)
-                    break;
-                uint32_t x[kMaxQ];
-                x[1] = j;
-                dfs_thread<2, DEND, ENUM, kThreadNW>(pr.lp, r64, rlo, D, x, cnt, ec);
+            if (DEND == 3 || pr.lp.free_from <= 2) { // block-uniform
+                // level 2 is the last or is counted in closed form: O(1) per level-1 vertex
+                for (;;) {
+                    const uint32_t j = atomicAdd(&s_j, 1u);
+                    if (j >= D)
+                        break;
+                    uint32_t x[kMaxQ];
+                    x[1] = j;
+                    dfs_thread<2, DEND, ENUM, kThreadNW>(pr.lp, r64, rlo, D, x, cnt, ec);
+                }
+            } else {
+                // one thread per (level-1, level-2) pair, so that threads get
+                // even shares whatever the level-1 vertices' candidate counts
+                const uint32_t n1 = D - j0, nw = (D + 63) >> 6;
+                uint32_t *s_cnt = s_pre; // free again once the rows are built
+                for (uint32_t i = threadIdx.x; i < n1; i += blockDim.x) {
+                    uint32_t x[kMaxQ];
+                    x[1] = j0 + i;
+                    const uint32_t lo2 = level_bound<2>(pr.lp, x);
+                    uint32_t c = 0;
+                    for (uint32_t k = lo2 >> 6; k < nw; ++k)
+                        c += (uint32_t)__popcll(cand_word<2, kThreadNW>(pr.lp, r64, rlo, D, lo2, x, k));
+                    s_cnt[i] = c;
+                }
+                __syncthreads();
+                if (threadIdx.x < 32)
+                    warp_excl_scan(s_cnt, n1, (int)threadIdx.x);
+                __syncthreads();
+                const uint32_t T = s_cnt[n1];
+                for (uint32_t t = threadIdx.x; t < T; t += blockDim.x) {
+                    uint32_t a = 0, b = n1; // last i with s_cnt[i] <= t
+                    while (b - a > 1) {
+                        const uint32_t mid = (a + b) >> 1;
+                        if (s_cnt[mid] <= t)
+                            a = mid;
+                        else
+                            b = mid;
+                    }
+                    uint32_t x[kMaxQ];
+                    x[1] = j0 + a;
+                    const uint32_t lo2 = level_bound<2>(pr.lp, x);
+                    uint32_t j = t - s_cnt[a];
+                    uint32_t k = lo2 >> 6;
+                    uint64_t w = cand_word<2, kThreadNW>(pr.lp, r64, rlo, D, lo2, x, k);
+                    for (uint32_t pc = (uint32_t)__popcll(w); j >= pc; pc = (uint32_t)__popcll(w)) {
+                        j -= pc;
+                        w = cand_word<2, kThreadNW>(pr.lp, r64, rlo, D, lo2, x, ++k);
+                    }
+                    x[2] = k * 64 + select64(w, j);
+                    dfs_thread<3, DEND, ENUM, kThreadNW>(pr.lp, r64, rlo, D, x, cnt, ec);
+                }
             }
         } else {
             const int glane = lane & (G - 1);
