@@ -11,6 +11,7 @@
 // lower_bound.
 #include <cmath>
 
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
 #include "internal.h"
@@ -180,72 +181,71 @@ __global__ void k_peel_init(const uint32_t *__restrict__ rp, int64_t n, uint32_t
     }
 }
 
-// Vertices with degree in [1, min_qdeg) are removed together
-// (bucket_scan window, subgraph_matching.cuh:66-109, 703).
-__global__ void k_peel_mark(const uint32_t *__restrict__ deg, uint8_t *alive, int64_t n, uint32_t min_qdeg,
-                            unsigned long long *removed) {
-    unsigned long long c = 0;
-    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t d = deg[v];
-        if (d >= 1 && d < min_qdeg) {
-            alive[v] = 0;
-            ++c;
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1)
-        c += __shfl_xor_sync(kFull, c, o);
-    if ((threadIdx.x & 31) == 0 && c)
-        atomicAdd(removed, c);
-}
-
-// Degree after dropping every edge with a removed endpoint
+// All peel rounds in one cooperative launch (every block resident; grid-wide
+// barriers between the phases of a round). A round removes together every
+// vertex whose degree is in [1, min_qdeg) (bucket_scan window,
+// subgraph_matching.cuh:66-109, 703) and lowers the degree of each surviving
+// neighbour once per removed neighbour, which leaves every degree equal to the
+// count of surviving neighbours -- what the reference's full recount gives
 // (remove_edges_connected_to_node + warp_detect_deleted_edges,
-// common_utils.cuh:99-133, 217-246).
-__global__ void k_peel_degree(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
-                              const uint8_t *__restrict__ alive, int64_t n, uint32_t *deg, RowChunk *chunks,
-                              unsigned *n_chunks, uint32_t cap) {
+// common_utils.cuh:99-133, 217-246). Rounds go on while one removes more than
+// 5% of n (subgraph_matching.cuh:699-758), so there are at most 21;
+// removed[r] counts round r (zeroed by the caller, kPeelMaxRounds entries).
+constexpr int kPeelMaxRounds = 32;
+
+__global__ void k_peel_fused(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n,
+                             uint32_t min_qdeg, uint32_t *deg, uint8_t *alive, uint32_t *list,
+                             unsigned long long *removed, int *rounds_out) {
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += warps * 32) {
-        const int64_t v = base + lane;
-        bool big = false;
-        uint32_t b = 0, e = 0;
-        if (v < n) {
-            if (!alive[v]) {
-                deg[v] = 0;
-            } else {
-                b = rp[v];
-                e = rp[v + 1];
-                if (e - b > kSerialMax) {
-                    big = true;
-                    deg[v] = 0; // the chunks add their counts
-                } else {
-                    uint32_t c = 0;
-                    for (uint32_t i = b; i < e; ++i)
-                        c += alive[col[i]];
-                    deg[v] = c;
-                }
+    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = nth >> 5;
+    const double limit = 0.05 * (double)n;
+    int round = 0;
+    for (;;) {
+        unsigned long long *cnt = removed + round;
+        // mark: threads of a warp take 32 consecutive vertices; one atomic per warp
+        for (int64_t base = warp * 32; base < n; base += nwarps * 32) {
+            const int64_t v = base + lane;
+            bool out = false;
+            if (v < n) {
+                const uint32_t d = deg[v];
+                out = d >= 1 && d < min_qdeg;
+                if (out)
+                    alive[v] = 0;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, out);
+            if (!bal)
+                continue;
+            unsigned long long at = 0;
+            if (lane == 0)
+                at = atomicAdd(cnt, (unsigned long long)__popc(bal));
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (out)
+                list[at + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)v;
+        }
+        grid.sync();
+        const unsigned long long R = *(volatile unsigned long long *)cnt;
+        // lower the surviving neighbours' degrees: a warp per removed vertex
+        for (unsigned long long i = (unsigned long long)warp; i < R; i += (unsigned long long)nwarps) {
+            const uint32_t w = list[i];
+            if (lane == 0)
+                deg[w] = 0;
+            const uint32_t b = rp[w], e = rp[w + 1];
+            for (uint32_t k = b + lane; k < e; k += 32) {
+                const uint32_t u = col[k];
+                if (alive[u])
+                    atomicSub(&deg[u], 1u);
             }
         }
-        push_chunks(big, (uint32_t)v, b, e, chunks, n_chunks, cap, lane);
+        grid.sync();
+        ++round;
+        if (!((double)R > limit) || round >= kPeelMaxRounds)
+            break;
     }
-}
-
-__global__ void k_peel_chunks(const uint32_t *__restrict__ col, const uint8_t *__restrict__ alive,
-                              const RowChunk *__restrict__ chunks, const unsigned *__restrict__ n_chunks,
-                              uint32_t cap, uint32_t *deg) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    const uint32_t nc = min(*n_chunks, cap);
-    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc; c += warps) {
-        const RowChunk ch = chunks[c];
-        uint32_t k = 0;
-        for (uint32_t i = ch.b + lane; i < ch.e; i += 32)
-            k += alive[col[i]];
-        k = __reduce_add_sync(kFull, k);
-        if (lane == 0 && k)
-            atomicAdd(&deg[ch.row], k);
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        *rounds_out = round;
 }
 
 // ---- relabelling -----------------------------------------------------------
@@ -573,7 +573,7 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     const size_t mm = m > 0 ? (size_t)m : 1;
     size_t need = Carve::need({(size_t)nn * 4, (size_t)nn, (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4,
                                (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4, mm * 8, mm * 8,
-                               cap * sizeof(RowChunk), 16});
+                               cap * sizeof(RowChunk), 16, (size_t)nn * 4, kPeelMaxRounds * 8});
     BEEP_TRY(ctx->grow(ctx->scratch2, need));
     Carve cv(ctx->scratch2.ptr);
     uint32_t *deg = cv.take<uint32_t>(nn);
@@ -584,7 +584,9 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     uint32_t *new_deg = cv.take<uint32_t>(nn);
     uint64_t *ekeys = cv.take<uint64_t>(mm), *ekeys2 = cv.take<uint64_t>(mm);
     RowChunk *chunks = cv.take<RowChunk>(cap);
-    unsigned *d_nchunks = cv.take<unsigned>(4);
+    unsigned *d_nchunks = cv.take<unsigned>(4); // [0] chunk count, [2] peel rounds
+    uint32_t *peel_list = cv.take<uint32_t>(nn);
+    unsigned long long *peel_removed = cv.take<unsigned long long>(kPeelMaxRounds);
     const uint32_t ucap = (uint32_t)std::min<size_t>(cap, 0xffffffffu);
     BEEP_TRY(ctx->grow(ctx->counter, 64));
     unsigned long long *d_removed = ctx->counter.as<unsigned long long>();
@@ -596,32 +598,25 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
         ++ctx->launches;
     }
     BEEP_CUDA_TRY(cudaGetLastError());
-    // Iterated peel: loop while a round removes more than 5% of n
-    // (subgraph_matching.cuh:699-758).
-    int rounds = 0;
-    for (;;) {
-        unsigned long long removed = 0;
-        if (min_qdeg > 1 && n > 0) {
-            BEEP_CUDA_TRY(cudaMemsetAsync(d_removed, 0, 8, s));
-            k_peel_mark<<<gv, 256, 0, s>>>(deg, alive, n, (uint32_t)min_qdeg, d_removed);
-            ++ctx->launches;
-            BEEP_CUDA_TRY(cudaGetLastError());
-            BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, d_removed, 8, cudaMemcpyDeviceToHost, s));
-            BEEP_CUDA_TRY(cudaStreamSynchronize(s));
-            removed = ctx->h_pinned[0];
-            if (removed > 0) {
-                BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks, 0, 4, s));
-                k_peel_degree<<<gv, 256, 0, s>>>(rp, col, alive, n, deg, chunks, d_nchunks, ucap);
-                k_peel_chunks<<<ctx->num_sms * 8, 256, 0, s>>>(col, alive, chunks, d_nchunks, ucap, deg);
-                ctx->launches += 2;
-            }
-            BEEP_CUDA_TRY(cudaGetLastError());
-        }
-        ++rounds;
-        if (!((double)removed > 0.05 * (double)n))
-            break;
+    // Iterated peel, all rounds in one cooperative launch (no host round trip
+    // per round).
+    int *d_rounds = reinterpret_cast<int *>(d_nchunks + 2);
+    BEEP_CUDA_TRY(cudaMemsetAsync(d_rounds, 0, 4, s));
+    if (min_qdeg > 1 && n > 0) {
+        BEEP_CUDA_TRY(cudaMemsetAsync(peel_removed, 0, kPeelMaxRounds * 8, s));
+        int per_sm = 0;
+        BEEP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel_fused, 256, 0));
+        // two blocks per SM at most: enough threads for these elementwise
+        // phases, and room left for kernels of other streams
+        const int blocks = (int)std::max<int64_t>(
+            1, std::min<int64_t>((int64_t)std::min(std::max(per_sm, 1), 2) * ctx->num_sms, (n + 255) / 256));
+        uint32_t mq = (uint32_t)min_qdeg;
+        int64_t nn_arg = n;
+        void *args[] = {(void *)&rp, (void *)&col, (void *)&nn_arg, (void *)&mq, (void *)&deg, (void *)&alive,
+                        (void *)&peel_list, (void *)&peel_removed, (void *)&d_rounds};
+        BEEP_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_peel_fused, dim3(blocks), dim3(256), args, 0, s));
+        ++ctx->launches;
     }
-    v->peel_rounds = rounds;
     tr.mark("peel");
 
     // Relabel by priority.
@@ -641,10 +636,13 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
     BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ctx->scratch.ptr, tb, pkey, pkey2, pid, pid2, n, 0, hb, s));
     // number of vertices that kept an edge
+    ctx->h_pinned[1] = 0; // the copy below fills its low 4 bytes
     BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, d_alive, 8, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned + 1, d_rounds, 4, cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     const int64_t na = (int64_t)ctx->h_pinned[0];
     v->n = na;
+    v->peel_rounds = std::max(1, (int)(uint32_t)ctx->h_pinned[1]);
     tr.mark("order");
     BEEP_TRY(ctx->grow(v->row_ptr, (size_t)(na + 1) * 4));
     BEEP_TRY(ctx->grow(v->orig, (size_t)(na > 0 ? na : 1) * 4));
