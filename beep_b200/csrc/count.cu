@@ -714,10 +714,41 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
             ec.A = A;
             ec.root = r;
         }
-        for (uint32_t j = j0 + glane; j < D; j += G) {
-            uint32_t x[kMaxQ];
-            x[1] = j;
-            dfs_thread<2, DEND, ENUM, 1>(pr.lp, rows, rlo, D, x, cnt, ec);
+        if (DEND == 3 || pr.lp.free_from <= 2) { // group-uniform
+            for (uint32_t j = j0 + glane; j < D; j += G) {
+                uint32_t x[kMaxQ];
+                x[1] = j;
+                dfs_thread<2, DEND, ENUM, 1>(pr.lp, rows, rlo, D, x, cnt, ec);
+            }
+        } else {
+            // one lane per (level-1, level-2) pair (see k_medium)
+            const uint32_t n1 = D - j0;
+            uint32_t *s_cnt = s_pre[gid];
+            for (uint32_t i = glane; i < n1; i += G) {
+                uint32_t x[kMaxQ];
+                x[1] = j0 + i;
+                const uint32_t lo2 = level_bound<2>(pr.lp, x);
+                s_cnt[i] = (uint32_t)__popcll(cand_word<2, 1>(pr.lp, rows, rlo, D, lo2, x, 0));
+            }
+            __syncwarp(gmask);
+            group_excl_scan<G>(s_cnt, n1, glane, gmask);
+            __syncwarp(gmask);
+            const uint32_t T = s_cnt[n1];
+            for (uint32_t t = glane; t < T; t += G) {
+                uint32_t a = 0, b = n1;
+                while (b - a > 1) {
+                    const uint32_t mid = (a + b) >> 1;
+                    if (s_cnt[mid] <= t)
+                        a = mid;
+                    else
+                        b = mid;
+                }
+                uint32_t x[kMaxQ];
+                x[1] = j0 + a;
+                const uint32_t lo2 = level_bound<2>(pr.lp, x);
+                x[2] = select64(cand_word<2, 1>(pr.lp, rows, rlo, D, lo2, x, 0), t - s_cnt[a]);
+                dfs_thread<3, DEND, ENUM, 1>(pr.lp, rows, rlo, D, x, cnt, ec);
+            }
         }
         __syncwarp(gmask);
     }
