@@ -270,67 +270,71 @@ __device__ __forceinline__ uint32_t select64(uint64_t w, uint32_t j) {
 template <int P, int DEND, bool ENUM, int NW>
 __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, uint32_t rlo, uint32_t D,
                                            uint32_t (&x)[kMaxQ], unsigned long long &cnt, const EnumCtx &ec) {
-    const uint32_t lo = level_bound<P>(lp, x);
-    bool closed = false; // count this level's candidates as C(A, DEND - P)
-    if constexpr (!ENUM && DEND - P <= 4) {
-        if (suffix_applies<P, DEND>(lp, x, lo)) {
-            if (lp.free_back == 0) {
-                cnt += binom_le4(free_count_rootonly<P>(D, x, lo), DEND - P);
+    if constexpr (P >= DEND) {
+        return; // never called: the callers stop at the last position
+    } else {
+        const uint32_t lo = level_bound<P>(lp, x);
+        bool closed = false; // count this level's candidates as C(A, DEND - P)
+        if constexpr (!ENUM && DEND - P <= 4) {
+            if (suffix_applies<P, DEND>(lp, x, lo)) {
+                if (lp.free_back == 0) {
+                    cnt += binom_le4(free_count_rootonly<P>(D, x, lo), DEND - P);
+                    return;
+                }
+                closed = DEND - P >= 2; // one level: the leaf popcount below is the same
+            }
+        }
+        if constexpr (NW == 1) {
+            // one word: the candidate set stays in a register
+            uint64_t c = cand_word<P, 1>(lp, rows, rlo, D, lo, x, 0);
+            if (closed) {
+                cnt += binom_le4((uint32_t)__popcll(c), DEND - P);
                 return;
             }
-            closed = DEND - P >= 2; // one level: the leaf popcount below is the same
-        }
-    }
-    if constexpr (NW == 1) {
-        // one word: the candidate set stays in a register
-        uint64_t c = cand_word<P, 1>(lp, rows, rlo, D, lo, x, 0);
-        if (closed) {
-            cnt += binom_le4((uint32_t)__popcll(c), DEND - P);
+            if constexpr (P == DEND - 1) {
+                if constexpr (ENUM)
+                    emit_bits(ec, x, P, c, 0);
+                cnt += (unsigned long long)__popcll(c);
+            } else {
+                while (c) {
+                    const int b = __ffsll((long long)c) - 1;
+                    c &= c - 1;
+                    x[P] = (uint32_t)b;
+                    dfs_thread<P + 1, DEND, ENUM, 1>(lp, rows, rlo, D, x, cnt, ec);
+                }
+            }
             return;
         }
-        if constexpr (P == DEND - 1) {
-            if constexpr (ENUM)
-                emit_bits(ec, x, P, c, 0);
-            cnt += (unsigned long long)__popcll(c);
-        } else {
-            while (c) {
-                const int b = __ffsll((long long)c) - 1;
-                c &= c - 1;
-                x[P] = (uint32_t)b;
-                dfs_thread<P + 1, DEND, ENUM, 1>(lp, rows, rlo, D, x, cnt, ec);
+        const uint32_t k0 = lo >> 6, nw = min((uint32_t)NW, (D + 63) >> 6);
+        if (closed || P == DEND - 1) {
+            uint32_t A = 0;
+            for (uint32_t k = k0; k < nw; ++k) {
+                const uint64_t w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
+                if constexpr (ENUM)
+                    emit_bits(ec, x, P, w, k * 64);
+                A += (uint32_t)__popcll(w);
             }
-        }
-        return;
-    }
-    const uint32_t k0 = lo >> 6, nw = min((uint32_t)NW, (D + 63) >> 6);
-    if (closed || P == DEND - 1) {
-        uint32_t A = 0;
-        for (uint32_t k = k0; k < nw; ++k) {
-            const uint64_t w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
-            if constexpr (ENUM)
-                emit_bits(ec, x, P, w, k * 64);
-            A += (uint32_t)__popcll(w);
-        }
-        cnt += closed ? binom_le4(A, DEND - P) : (unsigned long long)A;
-        return;
-    }
-    if constexpr (P < DEND - 1 && NW > 1) {
-        // one call site per level; only the current word and its index live
-        // across the call (the next word is recomputed from the rows)
-        uint32_t k = k0;
-        if (k >= nw)
+            cnt += closed ? binom_le4(A, DEND - P) : (unsigned long long)A;
             return;
-        uint64_t w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
-        for (;;) {
-            while (!w) {
-                if (++k >= nw)
-                    return;
-                w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
+        }
+        if constexpr (P < DEND - 1 && NW > 1) {
+            // one call site per level; only the current word and its index live
+            // across the call (the next word is recomputed from the rows)
+            uint32_t k = k0;
+            if (k >= nw)
+                return;
+            uint64_t w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
+            for (;;) {
+                while (!w) {
+                    if (++k >= nw)
+                        return;
+                    w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
+                }
+                const int b = __ffsll((long long)w) - 1;
+                w &= w - 1;
+                x[P] = k * 64 + (uint32_t)b;
+                dfs_thread<P + 1, DEND, ENUM, NW>(lp, rows, rlo, D, x, cnt, ec);
             }
-            const int b = __ffsll((long long)w) - 1;
-            w &= w - 1;
-            x[P] = k * 64 + (uint32_t)b;
-            dfs_thread<P + 1, DEND, ENUM, NW>(lp, rows, rlo, D, x, cnt, ec);
         }
     }
 }
