@@ -455,6 +455,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--step-api", choices=["batch", "plain"], default="batch",
+                    help="count the step's patterns with one batched call or one beep_count per pattern")
     ap.add_argument("--reference-port", action="store_true", help="reference arm: use the CPU port")
     ap.add_argument("--reference-timeout", type=float, default=300.0)
     ap.add_argument("--reference-budget", type=float, default=150.0,
@@ -510,10 +512,20 @@ def main():
             g = B.Graph.from_device_csr(ctx, n, m, d_rp.data_ptr(), d_col.data_ptr())
         total = 0
         sts = []
-        for q in queries:
-            c, st = B.count(g, q, mode, options, ctx=ctx, stats=True)
-            total += c
-            sts.append(st)
+        if args.step_api == "batch":
+            # one planned call over every pattern: the views of both patterns
+            # are built, then all their count kernels run together
+            b = B.Batch(ctx)
+            for q in queries:
+                b.add(g, q, mode)
+            counts, st = b.run(options | B.OPT_NO_GRAPH, stats=True)
+            b.close()
+            total, sts = sum(counts), [st]
+        else:
+            for q in queries:
+                c, st = B.count(g, q, mode, options, ctx=ctx, stats=True)
+                total += c
+                sts.append(st)
         g.close()
         return total, sts
 
@@ -614,7 +626,9 @@ def main():
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": wl["desc"], "n": n, "m_directed": m, "patterns": wl["patterns"], "mode": wl["mode"],
                    "matches_per_step": per_step, "l2": "flushed (256 MB write) before every step",
-                   "step": "device CSR build + per-pattern peel/relabel + count"},
+                   "step": "device CSR build + per-pattern peel/relabel + count" +
+                           (", both patterns in one batched call (beep_batch, no CUDA graph)"
+                            if args.step_api == "batch" else ", one beep_count per pattern")},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * (n + 1) + 4 * m),
                 "d2h_bytes_per_step": 8 * len(queries) + 16, "ms_per_step": e_ms / args.steps,
                 "h2d_copy_ms": h2d_ms},
