@@ -517,73 +517,14 @@ __device__ __forceinline__ uint32_t search_steps(uint32_t x) { return 32u - (uin
 // slice is much longer than that part of A -- the usual case for domain
 // vertices of high degree. s_len[r] holds the slice length, with the top bit
 // set for the second direction.
-// Open-addressing hash of the domain list in shared memory: slot -> index
-// into A (kHashEmpty: free), at most half full, so a lookup is one or two
-// shared loads instead of a binary search's log D dependent ones.
-constexpr uint32_t kHashEmpty = 0xffffffffu;
-
-struct DomHash {
-    uint32_t *tab = nullptr; // nullptr: binary search in A instead
-    uint32_t mask = 0;
-    int shift = 32;
-};
-
-__device__ __forceinline__ uint32_t hash_slot(uint32_t key, int shift) { return (key * 2654435761u) >> shift; }
-
-// log2 of the table size for a domain of D entries (>= 2D slots, at least 2^lmin)
-__host__ __device__ inline int hash_log2(uint32_t D, int lmin) {
-    int l = lmin;
-    while ((1u << l) < 2u * D)
-        ++l;
-    return l;
-}
-
-__device__ __forceinline__ int hash_find(const DomHash &h, const uint32_t *A, uint32_t key) {
-    uint32_t slot = hash_slot(key, h.shift);
-    for (uint32_t probe = 0; probe <= h.mask; ++probe) {
-        const uint32_t t = h.tab[slot];
-        if (t == kHashEmpty)
-            return -1;
-        if (A[t] == key)
-            return (int)t;
-        slot = (slot + 1) & h.mask;
-    }
-    return -1;
-}
-
-// Only edges with an endpoint at index >= rlo are found (the rows below rlo
-// are not stored): in ascending order row i searches A[max(i + 1, rlo), D),
-// in descending order rows below rlo search nothing.
-//
-// Each row picks the cheaper direction: its list slice (c entries) searched
-// in A (shared memory: the hash, or a binary search), or the nA entries of A
-// it can meet searched in the list slice (global memory, nA * log c steps)
-// when the slice is much longer than that part of A -- the usual case for
-// domain vertices of high degree. s_len[r] holds the slice length, with the
-// top bit set for the second direction.
 template <int G, typename SetFn>
 __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const uint32_t *A, uint32_t D,
                                                 uint32_t rlo, uint32_t i0, uint32_t i1, uint32_t *s_hb,
                                                 uint32_t *s_pre, uint32_t *s_len, uint32_t tid, uint32_t nthr,
-                                                unsigned gmask, const DomHash &hash, SetFn set) {
+                                                unsigned gmask, SetFn set) {
     constexpr uint32_t kByA = 0x80000000u;
-    constexpr uint32_t kSpan = G == 0 ? 32u : (uint32_t)G; // lanes that take consecutive elements
     const uint32_t R = i1 - i0;
-    if (hash.tab) {
-        for (uint32_t k = tid; k <= hash.mask; k += nthr)
-            hash.tab[k] = kHashEmpty;
-        group_sync<G>(gmask);
-        for (uint32_t k = tid; k < D; k += nthr) {
-            uint32_t slot = hash_slot(A[k], hash.shift);
-            for (uint32_t probe = 0; probe <= hash.mask; ++probe) {
-                if (atomicCAS(&hash.tab[slot], kHashEmpty, k) == kHashEmpty)
-                    break;
-                slot = (slot + 1) & hash.mask;
-            }
-        }
-    }
-    // a hash lookup costs about as much as a global search step
-    const uint32_t logD = hash.tab ? 2u : search_steps(D);
+    const uint32_t logD = search_steps(D);
     for (uint32_t r = tid; r < R; r += nthr) {
         const uint32_t i = i0 + r;
         uint32_t hb, he, xb, xe, c = 0, work = 0, len = 0;
@@ -623,24 +564,8 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
     group_sync<G>(gmask);
     const uint32_t T = s_pre[R];
     for (uint32_t t = tid; t < T; t += nthr) {
-        // row of element t: the last r with s_pre[r] <= t. The lanes of a warp
-        // (group) hold consecutive elements: one shared binary search for the
-        // first of them, then each lane gallops forward from that row.
-        const uint32_t t0 = t - (tid & (kSpan - 1));
+        // row r: last with s_pre[r] <= t
         uint32_t lo = 0, hi = R;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_pre[mid] <= t0)
-                lo = mid;
-            else
-                hi = mid;
-        }
-        uint32_t step = 1;
-        while (lo + step < R && s_pre[lo + step] <= t) {
-            lo += step;
-            step <<= 1;
-        }
-        hi = min(lo + step, R);
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;
             if (s_pre[mid] <= t)
@@ -658,14 +583,7 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
                 set(i, k);
         } else {
             const uint32_t w = v.col[s_hb[lo] + (t - s_pre[lo])];
-            int k;
-            if (hash.tab) {
-                k = hash_find(hash, A, w);
-                if (k >= 0 && ((uint32_t)k < xb || (uint32_t)k >= xe))
-                    k = -1;
-            } else {
-                k = find_idx(A, xb, xe, w);
-            }
+            const int k = find_idx(A, xb, xe, w);
             if (k >= 0)
                 set(i, (uint32_t)k);
         }
@@ -757,9 +675,6 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
     __shared__ uint32_t s_hb[NG][MAXD];
     __shared__ uint32_t s_len[NG][MAXD];
     __shared__ uint32_t s_pre[NG][MAXD + 1];
-    __shared__ uint32_t s_hash[NG][2 * MAXD];
-    constexpr int kHashLog = MAXD >= 64 ? 7 : (MAXD >= 32 ? 6 : (MAXD >= 16 ? 5 : 4));
-    static_assert((1 << kHashLog) == 2 * MAXD, "hash table of 2 * MAXD slots");
     const int gid = threadIdx.x / G, glane = threadIdx.x % G;
     const int lane = threadIdx.x & 31;
     const unsigned gmask = G == 32 ? kFull : (((1u << G) - 1u) << (lane & ~(G - 1)));
@@ -792,8 +707,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_small(const PairDev *__res
         __syncwarp(gmask);
         if (rlo < D)
             build_rows_flat<G>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb[gid], s_pre[gid], s_len[gid], (uint32_t)glane,
-                               (uint32_t)G, gmask, DomHash{s_hash[gid], (1u << kHashLog) - 1u, 32 - kHashLog},
-                               [&](uint32_t i, uint32_t k) {
+                               (uint32_t)G, gmask, [&](uint32_t i, uint32_t k) {
                                    if (i >= rlo)
                                        atomicOr((unsigned long long *)&rows[i - rlo], 1ull << k);
                                    if (k >= rlo)
@@ -866,9 +780,7 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? 2 : 1) k_medium(
     uint32_t *s_hb = sm + pad;
     uint32_t *s_pre = sm + 2 * pad;
     uint32_t *s_len = sm + 3 * pad;
-    const int hlog = hash_log2(maxD, 5);
-    const DomHash hash{sm + 4 * pad, (1u << hlog) - 1u, 32 - hlog};
-    uint32_t *rows = sm + 4 * pad + (1u << hlog);
+    uint32_t *rows = sm + 4 * pad;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
     EnumCtx ec;
@@ -909,7 +821,7 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? 2 : 1) k_medium(
             if constexpr (G == 0) {
                 unsigned long long *r64 = reinterpret_cast<unsigned long long *>(rows);
                 build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, s_len, threadIdx.x, blockDim.x,
-                                   kFull, hash, [&](uint32_t i, uint32_t k) {
+                                   kFull, [&](uint32_t i, uint32_t k) {
                                        if (i >= rlo)
                                            atomicOr(&r64[(size_t)(i - rlo) * kThreadNW + (k >> 6)], 1ull << (k & 63));
                                        if (k >= rlo)
@@ -917,7 +829,7 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? 2 : 1) k_medium(
                                    });
             } else {
                 build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, s_len, threadIdx.x, blockDim.x,
-                                   kFull, hash, [&](uint32_t i, uint32_t k) {
+                                   kFull, [&](uint32_t i, uint32_t k) {
                                        if (i >= rlo)
                                            atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
                                        if (k >= rlo)
@@ -1065,7 +977,7 @@ __global__ void __launch_bounds__(512) k_large_rows(const PairDev *__restrict__ 
             A = sA;
         }
         if (rlo < D) // block-uniform
-            build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, i0, i1, s_hb, s_pre, s_len, threadIdx.x, blockDim.x, kFull, DomHash{},
+            build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, i0, i1, s_hb, s_pre, s_len, threadIdx.x, blockDim.x, kFull,
                                [&](uint32_t i, uint32_t k) {
                                    if (i >= rlo)
                                        atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
@@ -1699,7 +1611,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         // 32-bit words per row: 8 (4 x 64 bits) in the thread-mode sub-tier
         const uint32_t W = sub == 0 ? 8u : (maxD + 31) / 32;
         const size_t pad = (maxD + 4) & ~3u;
-        const size_t smem = (4 * pad + ((size_t)1 << hash_log2(maxD, 5)) + (size_t)maxD * W) * 4;
+        const size_t smem = (4 * pad + (size_t)maxD * W) * 4;
         const int block = sub == 0 ? 256 : 1024;
         const int per_sm = std::max(1, (int)std::min<size_t>(2048 / block, (200 * 1024) / (smem + 1024)));
         uint32_t first = 0;
