@@ -36,6 +36,7 @@ OPT_TIMING = 1 << 1
 OPT_NO_VIEW_CACHE = 1 << 2
 OPT_ALG_BYTES = 1 << 3
 OPT_NO_GRAPH = 1 << 4
+OPT_SERIAL_TIERS = 1 << 5
 
 
 class BeepError(RuntimeError):

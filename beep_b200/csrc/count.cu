@@ -1684,7 +1684,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
 }
 
 namespace {
-beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::vector<std::pair<cudaEvent_t, cudaEvent_t>> *ev,
+beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats &st,
+                  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> *ev,
                   std::vector<double *> *sinks) {
     cudaStream_t s = ctx->stream;
     const uint32_t np = lp->np;
@@ -1697,7 +1698,7 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::ve
         have_medium |= r.kind == LaunchRec::kMedium;
         have_small |= r.kind == LaunchRec::kSmall;
     }
-    const bool fork = have_medium || have_small;
+    const bool fork = (have_medium || have_small) && !serial;
     if (fork) {
         BEEP_TRY(ctx->ensure_side());
         BEEP_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
@@ -1706,9 +1707,9 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, beep_stats &st, std::ve
     }
     for (auto &r : lp->recs) {
         cudaStream_t rs = s;
-        if (r.kind == LaunchRec::kMedium)
+        if (fork && r.kind == LaunchRec::kMedium)
             rs = ctx->side[0];
-        else if (r.kind == LaunchRec::kSmall)
+        else if (fork && r.kind == LaunchRec::kSmall)
             rs = ctx->side[1];
         cudaEvent_t a = nullptr, b = nullptr;
         if (timing && r.sink) {
@@ -1793,7 +1794,7 @@ beep_status capture_plan(Ctx *ctx, LaunchPlan *lp) {
     std::memset(&scratch_st, 0, sizeof(scratch_st));
     cudaGraph_t graph = nullptr;
     BEEP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    beep_status rc = issue(ctx, lp, false, scratch_st, nullptr, nullptr);
+    beep_status rc = issue(ctx, lp, false, false, scratch_st, nullptr, nullptr);
     cudaError_t ce = cudaMemcpyAsync(lp->h_counts, lp->d_counts, (lp->np + 4) * 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamEndCapture(s, &graph);
     if (rc != BEEP_OK) {
@@ -1830,7 +1831,7 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
             st.kernel_launches += r.kind != LaunchRec::kMemset;
     } else {
         st.kernel_launches = lp->st.kernel_launches;
-        BEEP_TRY(issue(ctx, lp, timing, st, &ev, &sinks));
+        BEEP_TRY(issue(ctx, lp, timing, (options & BEEP_OPT_SERIAL_TIERS) != 0, st, &ev, &sinks));
         BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, (lp->np + 4) * 8, cudaMemcpyDeviceToHost, s));
     }
     if (timing)
@@ -1892,7 +1893,7 @@ beep_status launch_plan_async(Ctx *ctx, LaunchPlan *lp) {
     }
     beep_stats st;
     std::memset(&st, 0, sizeof(st));
-    BEEP_TRY(issue(ctx, lp, false, st, nullptr, nullptr));
+    BEEP_TRY(issue(ctx, lp, false, false, st, nullptr, nullptr));
     BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, (lp->np + 4) * 8, cudaMemcpyDeviceToHost, ctx->stream));
     return BEEP_OK;
 }

@@ -36,6 +36,8 @@ UNIT = "matches/s"
 WORKLOADS = {
     "c2": {"desc": "plain-mid: R-MAT s20 ef3 seed 7; 4-clique + diamond (sgm)",
            "graph": ("rmat", (20, 3, 0.57, 0.19, 0.19, 7)), "patterns": ["k4", "diamond"], "mode": "sgm"},
+    "c3": {"desc": "plain-large: R-MAT s22 ef28 seed 11; 5-clique + 4-wheel (sgm)",
+           "graph": ("rmat", (22, 28, 0.57, 0.19, 0.19, 11)), "patterns": ["k5", "w5"], "mode": "sgm"},
     "c1": {"desc": "plain-small: ER G(4096, 0.004) seed 1; triangle (sgc)",
            "graph": ("er", (4096, 0.004, 1)), "patterns": ["triangle"], "mode": "sgc"},
     "c4": {"desc": "batched: Chung-Lu graphs (exponent 2.1, seed 13) x the 15 central 4-5-vertex patterns (sgm)"},
@@ -529,9 +531,9 @@ def main():
         g.close()
         return total, sts
 
-    def timed(host: bool, steps: int):
+    def timed(host: bool, steps: int, options: int = 0):
         for _ in range(args.warmup):
-            step(host)
+            step(host, options)
         torch.cuda.synchronize()
         barrier(world)
         launches0 = ctx.kernel_launches()
@@ -543,8 +545,7 @@ def main():
             total, allst = 0, []
             for _ in range(steps):
                 flush.fill_(1)
-                # per-kernel CUDA events on the library's stream (cheap) in the device-resident run
-                t, sts = step(host, 0 if host else B.OPT_TIMING)
+                t, sts = step(host, options)
                 total += t
                 allst.append(sts)
             e1.record(stream)
@@ -592,6 +593,13 @@ def main():
     t0 = time.perf_counter()
     g.close()
     host_ms["graph_destroy"] = (time.perf_counter() - t0) * 1e3
+    # Per-kernel times. In the timed steps the kernel tiers overlap on side
+    # streams, so an event pair around one kernel measures the overlap, not the
+    # kernel. These steps run the same work with the tiers one after another
+    # (BEEP_OPT_SERIAL_TIERS) and an event pair around every launch, so each
+    # kernel's time is its own and the shares compare with the ncu launch list.
+    ser_steps = max(1, min(args.steps, 10))
+    _, _, allst, _ = timed(False, ser_steps, B.OPT_TIMING | B.OPT_SERIAL_TIERS)
     # adjacency bytes per tier, from one untimed pass (identical every step)
     _, byte_sts = step(False, B.OPT_ALG_BYTES)
     for sts in allst:
@@ -634,8 +642,9 @@ def main():
                 "h2d_copy_ms": h2d_ms},
         "gpu_launches": int(launches),
         "host_calls_ms": host_ms,
-        "phases_ms_per_step": {"prep": prep_ms / args.steps, "count": count_ms / args.steps,
-                               **{k: v[0] / args.steps for k, v in agg.items()}},
+        "phases_ms_per_step": {"prep": prep_ms / ser_steps, "count": count_ms / ser_steps,
+                               **{k: v[0] / ser_steps for k, v in agg.items()},
+                               "note": f"{ser_steps} extra steps with the kernel tiers serialised and timed per launch"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": profiled_traffic().get({"small": "k_small", "medium": "k_medium",

@@ -152,7 +152,11 @@ enum {
     /* Drop the graph's cached peeled/ordered views before running. */
     BEEP_OPT_NO_VIEW_CACHE = 1u << 2,
     /* Compute the adjacency bytes of the searched roots (an extra pass). */
-    BEEP_OPT_ALG_BYTES = 1u << 3
+    BEEP_OPT_ALG_BYTES = 1u << 3,
+    /* Launch the kernel tiers one after another on the call's stream instead
+     * of overlapping them on side streams (with BEEP_OPT_TIMING: per-kernel
+     * times that are each kernel's own). */
+    BEEP_OPT_SERIAL_TIERS = 1u << 5
 };
 
 typedef struct beep_stats {
