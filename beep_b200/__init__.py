@@ -71,6 +71,7 @@ class PlanInfo(ctypes.Structure):
         ("max_qdeg", ctypes.c_int32),
         ("aut_order", ctypes.c_int32),
         ("restricted", ctypes.c_int32),
+        ("central", ctypes.c_int32),
     ]
 
 
@@ -117,6 +118,10 @@ class Stats(ctypes.Structure):
         ("small_bytes", ctypes.c_uint64),
         ("medium_bytes", ctypes.c_uint64),
         ("large_bytes", ctypes.c_uint64),
+        ("roots_general", ctypes.c_int64),
+        ("general_ms", ctypes.c_double),
+        ("general_launches", ctypes.c_int32),
+        ("pad0", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -373,6 +378,7 @@ class Query:
             "max_qdeg": p.max_qdeg,
             "aut_order": p.aut_order,
             "restricted": p.restricted,
+            "central": p.central,
         }
 
     def close(self) -> None:

@@ -1034,9 +1034,155 @@ __global__ void __launch_bounds__(256) k_large_dfs(const PairDev *__restrict__ p
 }
 
 // ---------------------------------------------------------------------------
+// queries without a central vertex: list walker. The neighbourhood bitmaps
+// above need every position adjacent to the root; here a thread takes one
+// (root, level-1 vertex) task and walks the rest of the matching order over
+// the view's sorted neighbour lists: a position's candidates are the entries
+// of the shortest list among its back-edge positions (the root included)
+// that lie in every other such list, are not used yet and follow every
+// position the symmetry chain puts before it. Counts full matches (sgm).
+// ---------------------------------------------------------------------------
+struct GenRegs {
+    ViewDev v;
+    uint32_t back[kMaxQ]; // bits q >= 1
+    uint32_t sym[kMaxQ];  // bits s >= 1
+    uint32_t adj0, sym0;  // bit p: position p adjacent to / after position 0
+    int32_t order[kMaxQ];
+    int32_t K;
+    EnumDev en;
+};
+
+__device__ __forceinline__ void load_gen(const PairDev &pd, GenRegs &g) {
+    g.v = pd.v;
+#pragma unroll
+    for (int i = 0; i < kMaxQ; ++i) {
+        g.back[i] = pd.pl.back[i];
+        g.sym[i] = pd.pl.sym[i];
+        g.order[i] = pd.pl.order[i];
+    }
+    g.adj0 = pd.pl.adj0;
+    g.sym0 = pd.pl.sym0;
+    g.K = pd.pl.K;
+    g.en = pd.en;
+}
+
+// one tuple, in query-vertex order and input ids
+__device__ __forceinline__ void gen_emit(const GenRegs &g, const uint32_t (&x)[kMaxQ], int P, uint32_t w) {
+    if (g.en.out == nullptr || *(volatile unsigned long long *)g.en.n >= g.en.k)
+        return;
+    const unsigned long long slot = atomicAdd(g.en.n, 1ull);
+    if (slot >= g.en.k)
+        return;
+    int32_t *t = g.en.out + slot * (unsigned long long)g.K;
+    for (int q = 0; q < P; ++q)
+        t[g.order[q]] = (int32_t)g.v.orig[x[q]];
+    t[g.order[P]] = (int32_t)g.v.orig[w];
+}
+
+template <int P, int DEND, bool ENUM>
+__device__ void gen_walk(const GenRegs &g, uint32_t (&x)[kMaxQ], unsigned long long &cnt) {
+    if constexpr (P >= DEND) {
+        return;
+    } else {
+        const uint32_t bset = g.back[P] | ((g.adj0 >> P) & 1u); // bit 0: the root
+        uint32_t lo = 0;
+#pragma unroll
+        for (int q = 1; q < P; ++q)
+            if (g.sym[P] >> q & 1u)
+                lo = max(lo, x[q] + 1);
+        if (g.sym0 >> P & 1u)
+            lo = max(lo, x[0] + 1);
+        int qd = 0;
+        uint32_t db = 0, de = 0, best = 0xffffffffu;
+#pragma unroll
+        for (int q = 0; q < P; ++q)
+            if (bset >> q & 1u) {
+                const uint32_t b = g.v.rp[x[q]], e = g.v.rp[x[q] + 1];
+                if (e - b < best) {
+                    best = e - b;
+                    qd = q;
+                    db = b;
+                    de = e;
+                }
+            }
+        for (uint32_t k = lower_bound_g(g.v.col, db, de, lo); k < de; ++k) {
+            const uint32_t w = g.v.col[k];
+            bool ok = true;
+#pragma unroll
+            for (int q = 0; q < P; ++q)
+                ok = ok && x[q] != w;
+#pragma unroll
+            for (int q = 0; q < P; ++q)
+                if (ok && q != qd && (bset >> q & 1u))
+                    ok = contains_g(g.v.col, g.v.rp[x[q]], g.v.rp[x[q] + 1], w);
+            if (!ok)
+                continue;
+            if constexpr (P == DEND - 1) {
+                if constexpr (ENUM)
+                    gen_emit(g, x, P, w);
+                ++cnt;
+            } else {
+                x[P] = w;
+                gen_walk<P + 1, DEND, ENUM>(g, x, cnt);
+            }
+        }
+    }
+}
+
+// Items of one depth; tstart[i] - tstart[0] = first task of item i
+// (tstart[n] - tstart[0] tasks in all). Warps take 32 tasks at a time.
+template <int DEND, bool ENUM>
+__global__ void __launch_bounds__(256) k_general(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ items,
+                                                 const uint32_t *__restrict__ tstart, uint32_t nitems,
+                                                 unsigned *cursor) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t base0 = tstart[0], total = tstart[nitems] - base0;
+    GenRegs g;
+    uint32_t cur = 0xffffffffu;
+    unsigned long long cnt = 0, *count_ptr = nullptr;
+    for (;;) {
+        uint32_t t0 = 0;
+        if (lane == 0)
+            t0 = atomicAdd(cursor, 32u);
+        t0 = __shfl_sync(kFull, t0, 0);
+        if (t0 >= total)
+            break;
+        const uint32_t t = t0 + (uint32_t)lane;
+        if (t >= total)
+            continue;
+        const uint32_t b = find_batch(tstart, nitems, t + base0);
+        const uint64_t it = items[b];
+        const uint32_t p = item_pair(it), r = item_root(it);
+        if (p != cur) {
+            if (cnt)
+                atomicAdd(count_ptr, cnt);
+            cnt = 0;
+            cur = p;
+            load_gen(pairs[p], g);
+            count_ptr = pairs[p].count;
+        }
+        const uint32_t j0 = (g.sym0 >> 1 & 1u) ? g.v.split[r] : 0u;
+        uint32_t x[kMaxQ];
+        x[0] = r;
+        x[1] = g.v.col[g.v.rp[r] + j0 + (t + base0 - tstart[b])];
+        gen_walk<2, DEND, ENUM>(g, x, cnt);
+    }
+    if (cnt)
+        atomicAdd(count_ptr, cnt);
+}
+
+// task counts (D - j0) of listed items
+__global__ void k_gen_tasks(const uint32_t *__restrict__ D, const uint32_t *__restrict__ j0, uint32_t n,
+                            uint32_t *tasks) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        tasks[i] = D[i] - j0[i];
+}
+
+// ---------------------------------------------------------------------------
 // root classification over the vertices of every pair (flattened index)
 // ---------------------------------------------------------------------------
-constexpr int kTiers = 4;   // 1 small (D <= 64), 2 medium (<= 256), 3 medium (<= 1024), 4 large
+constexpr int kTiers = 5;   // 1 small (D <= 64), 2 medium (<= 256), 3 medium (<= 1024), 4 large,
+                            // 5 list walker (queries without a central vertex)
 constexpr int kDepths = 11; // dend 0..10
 
 __device__ __forceinline__ uint32_t find_pair(const uint64_t *__restrict__ offs, uint32_t npairs, uint64_t t) {
@@ -1063,7 +1209,7 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
     for (int i = threadIdx.x; i < kDepths; i += blockDim.x)
         s_tiny[i] = 0;
     __syncthreads();
-    uint32_t mx[kTiers] = {0, 0, 0, 0};
+    uint32_t mx[kTiers] = {0, 0, 0, 0, 0};
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t p = find_pair(offs, npairs, t);
         const uint32_t r = (uint32_t)(t - offs[p]);
@@ -1082,9 +1228,16 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
         // roots: degree in [max_qdeg, cap) (subgraph_matching.cuh:1086-1098),
         // enough domain vertices for the other dend-1 positions and at least
         // one level-1 vertex
-        if (deg >= pd.min_deg && deg < pd.cap_deg && D + 1 >= (uint32_t)pd.pl.dend && j0 < D &&
-            (pd.shard_mod <= 1 || pd.v.orig[r] % pd.shard_mod == pd.shard_rem))
+        const bool root_ok = deg >= pd.min_deg && deg < pd.cap_deg && j0 < D &&
+                             (pd.shard_mod <= 1 || pd.v.orig[r] % pd.shard_mod == pd.shard_rem);
+        if (!pd.pl.central) {
+            if (root_ok) {
+                tc = 5;
+                D -= j0; // level-1 tasks of the list walker
+            }
+        } else if (root_ok && D + 1 >= (uint32_t)pd.pl.dend) {
             tc = D <= kSmallMaxD ? 1 : (D <= kMediumAMaxD ? 2 : (D <= kMediumMaxD ? 3 : 4));
+        }
         tier[t] = tc;
         dom[t] = D;
         if (tc) {
@@ -1147,7 +1300,7 @@ __global__ void k_alg_bytes(const PairDev *__restrict__ pairs, const uint64_t *_
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < N; t += warps) {
         const int tc = tier[t];
-        if (!tc)
+        if (!tc || tc == 5) // the list walker has no bitmap tier
             continue;
         const uint32_t p = find_pair(offs, npairs, t);
         PairRegs pr;
@@ -1194,6 +1347,19 @@ beep_status launch_small(int dend, int group, int grid, cudaStream_t s, const Pa
             k_small<D, ENUM, 8, kTinyMaxD><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n);                      \
         else                                                                                                       \
             k_small<D, ENUM, 32, kSmallMaxD><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n);                    \
+        break;
+    BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
+#undef BEEP_CASE
+    BEEP_CUDA_TRY(cudaGetLastError());
+    return BEEP_OK;
+}
+
+template <bool ENUM>
+beep_status launch_general(int dend, int grid, cudaStream_t s, const PairDev *pairs, const uint64_t *items,
+                           const uint32_t *tstart, uint32_t n, unsigned *cursor) {
+#define BEEP_CASE(D)                                                                                               \
+    case D:                                                                                                        \
+        k_general<D, ENUM><<<grid, 256, 0, s>>>(pairs, items, tstart, n, cursor);                                   \
         break;
     BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
 #undef BEEP_CASE
@@ -1273,7 +1439,8 @@ struct Timer {
 // captured once into a CUDA graph (capture_plan) and relaunched.
 // ---------------------------------------------------------------------------
 struct LaunchRec {
-    enum Kind { kSmall, kMedium, kLargeRows, kLargeDfs, kMemset } kind;
+    enum Kind { kSmall, kMedium, kLargeRows, kLargeDfs, kGeneral, kMemset } kind;
+    const uint32_t *tstart = nullptr; // list walker: task prefix of the items
     int dend = 0, grid = 0, block = 0;
     int group = 32; // small tier: lanes per root
     size_t smem = 0;
@@ -1414,7 +1581,11 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     BEEP_CUDA_TRY(cudaMemcpyAsync(lp->d_offs, offs.data(), (np + 1) * 8, cudaMemcpyHostToDevice, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(d_misc, 0, 256 * 4, s));
     const int gv = std::max(1, (int)std::min<uint64_t>((N + 255) / 256, (uint64_t)ctx->num_sms * 32));
-    k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, lp->d_tier, d_dom, d_misc, d_misc + 4,
+    // d_misc: [0, 8) largest domain per tier, [8, 8 + kTiers * kDepths) roots
+    // per (tier, depth), [64, 64 + kDepths) tiny small-tier roots per depth,
+    // [80] selection count
+    static_assert(8 + kTiers * kDepths <= 64, "d_misc layout");
+    k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, lp->d_tier, d_dom, d_misc, d_misc + 8,
                                   d_misc + 64);
     BEEP_CUDA_TRY(cudaGetLastError());
     st.kernel_launches += 1;
@@ -1422,7 +1593,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     BEEP_CUDA_TRY(cudaMemcpyAsync(h_misc, d_misc, sizeof(h_misc), cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     const unsigned *tier_max = h_misc;
-    const unsigned *tier_depth = h_misc + 4;
+    const unsigned *tier_depth = h_misc + 8;
     const unsigned *tiny_depth = h_misc + 64;
     uint32_t tier_n[kTiers];
     for (int k = 0; k < kTiers; ++k) {
@@ -1433,7 +1604,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     st.roots_small = tier_n[0];
     st.roots_medium = (int64_t)tier_n[1] + tier_n[2];
     st.roots_large = tier_n[3];
-    st.roots = st.roots_small + st.roots_medium + st.roots_large;
+    st.roots_general = tier_n[4];
+    st.roots = st.roots_small + st.roots_medium + st.roots_large + st.roots_general;
     tr.mark("classify");
     uint32_t next_cursor = 0;
     auto cursor = [&]() -> unsigned * { return lp->d_cursors + (next_cursor++ % lp->ncursors); };
@@ -1664,6 +1836,44 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             }
         }
     }
+    // list walker (queries without a central vertex): tasks = level-1 vertices
+    if (tier_n[4] > 0) {
+        uint64_t *list = nullptr;
+        BEEP_TRY(make_list(4, list));
+        const uint32_t nl = tier_n[4];
+        uint32_t *tasks, *tstart;
+        BEEP_TRY(lp->alloc(tasks, nl));
+        BEEP_TRY(lp->alloc(tstart, (size_t)nl + 1));
+        k_gather_dom<<<std::max(1u, std::min(nl / 256 + 1, 1024u)), 256, 0, s>>>(lp->d_pairs, list, nl, d_keys,
+                                                                               d_sel);
+        k_gen_tasks<<<std::max(1u, std::min(nl / 256 + 1, 1024u)), 256, 0, s>>>(d_keys, d_sel, nl, tasks);
+        st.kernel_launches += 2;
+        BEEP_CUDA_TRY(cudaGetLastError());
+        size_t tb = 0;
+        BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, tasks, tstart, nl + 1, s));
+        BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
+        // tasks[nl] is not written: scan nl entries, then the total into tstart[nl]
+        BEEP_CUDA_TRY(cub::DeviceScan::InclusiveSum(ctx->scratch.ptr, tb, tasks, tstart + 1, nl, s));
+        BEEP_CUDA_TRY(cudaMemsetAsync(tstart, 0, 4, s));
+        uint32_t first = 0;
+        for (int d = 3; d < kDepths; ++d) {
+            const uint32_t cnt = tier_depth[4 * kDepths + d];
+            if (!cnt)
+                continue;
+            LaunchRec r;
+            r.kind = LaunchRec::kGeneral;
+            r.dend = d;
+            r.grid = ctx->num_sms * 8;
+            r.block = 256;
+            r.items = list + first;
+            r.tstart = tstart + first;
+            r.n = cnt;
+            r.cursor = cursor();
+            r.sink = &st.general_ms;
+            lp->recs.push_back(r);
+            first += cnt;
+        }
+    }
     // shared-memory opt-ins are host calls: done here, never inside a capture
     for (auto &r : lp->recs)
         if (r.kind == LaunchRec::kMedium) {
@@ -1752,6 +1962,13 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats
 #undef BEEP_CASE
             BEEP_CUDA_TRY(cudaGetLastError());
             st.medium_launches++;
+            break;
+        case LaunchRec::kGeneral:
+            if (lp->enumerate)
+                BEEP_TRY(launch_general<true>(r.dend, r.grid, rs, lp->d_pairs, r.items, r.tstart, r.n, r.cursor));
+            else
+                BEEP_TRY(launch_general<false>(r.dend, r.grid, rs, lp->d_pairs, r.items, r.tstart, r.n, r.cursor));
+            st.general_launches++;
             break;
         case LaunchRec::kSmall:
             if (lp->enumerate)
@@ -1863,7 +2080,9 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
         st.medium_ms = lp->st.medium_ms;
         st.large_encode_ms = lp->st.large_encode_ms;
         st.large_dfs_ms = lp->st.large_dfs_ms;
+        st.general_ms = lp->st.general_ms;
         lp->st.small_ms = lp->st.medium_ms = lp->st.large_encode_ms = lp->st.large_dfs_ms = 0;
+        lp->st.general_ms = 0;
     }
     for (size_t i = 0; i < ncounts; ++i)
         counts[i] = 0;
@@ -2173,6 +2392,8 @@ extern "C" beep_status beep_count_noalloc(int device, void *cuda_stream, int64_t
     if (mode == BEEP_MODE_SGC && plan.info.unmat)
         return fail(BEEP_ERR_UNSUPPORTED, "sgc with an unmaterialised last level depends on the reference's priority "
                                           "order, which needs the peeled and relabelled graph: use beep_count");
+    if (!plan.dev.central)
+        return fail(BEEP_ERR_UNSUPPORTED, "queries without a central vertex: use beep_count");
     DevPlan pl = plan.dev;
     pl.asc = 1; // vertex ids ascending are the priority order here
     cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);

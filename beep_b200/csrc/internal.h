@@ -70,6 +70,10 @@ struct DevPlan {
     int32_t free_from;       // positions [free_from, dend) share one back-edge set and form a symmetry chain
     uint32_t free_back;      // that back-edge set (bits q >= 1; 0: only the root)
     int32_t rows_needed;     // adjacency rows the DFS reads: 0 none, 1 only position 1's, 2 any
+    int32_t central;         // position 0 adjacent to every position (else: list walker)
+    uint32_t adj0;           // bit p: position p is adjacent to position 0
+    uint32_t sym0;           // bit p: position p must follow position 0
+    int32_t pad3;
 };
 
 struct QueryPlan {

@@ -198,10 +198,19 @@ beep_status compile_plan(int32_t qn, const std::vector<int32_t> &rp, const std::
             adj_prev |= P.qedge[e] == qn - 2;
         P.unmat = adj_prev ? 0 : 1;
     }
-    // The DFS assumes position 0 is adjacent to every position (README.md:51-53).
-    for (int i = 1; i < qn; ++i)
-        if (P.qedge_ptr[i + 1] == P.qedge_ptr[i] || P.qedge[P.qedge_ptr[i]] != 0)
-            return fail(BEEP_ERR_UNSUPPORTED, "query has no central vertex adjacent to all others");
+    // The bitmap DFS needs position 0 adjacent to every position
+    // (README.md:51-53); other queries go to the list walker, which counts
+    // full matches only.
+    P.central = 1;
+    for (int i = 1; i < qn; ++i) {
+        if (P.qedge_ptr[i + 1] == P.qedge_ptr[i])
+            return fail(BEEP_ERR_UNSUPPORTED, "query is not connected");
+        if (P.qedge[P.qedge_ptr[i]] != 0)
+            P.central = 0;
+    }
+    if (!P.central && P.unmat)
+        return fail(BEEP_ERR_UNSUPPORTED,
+                    "sgc prefix counts (last position not adjacent to the one before) need a central query");
 
     // Kernel view of the plan.
     DevPlan D;
@@ -226,7 +235,7 @@ beep_status compile_plan(int32_t qn, const std::vector<int32_t> &rp, const std::
     // Restricted search: if position 1 follows the root and every later
     // position follows position 1 through the constraint chain, all matched
     // vertices follow the root, so only the root's later neighbours matter.
-    bool restricted = D.pos1_after_root != 0;
+    bool restricted = D.pos1_after_root != 0 && P.central;
     std::array<uint32_t, kMaxQ> after{}; // positions that p must follow (transitively)
     for (int p = 1; p < qn; ++p) {
         uint32_t a = D.sym[p];
@@ -262,6 +271,15 @@ beep_status compile_plan(int32_t qn, const std::vector<int32_t> &rp, const std::
     for (int p = 2; p < D.dend; ++p)
         read |= D.back[p];
     D.rows_needed = read == 0 ? 0 : (read == 2u ? 1 : 2);
+    D.central = P.central;
+    for (int p = 1; p < qn; ++p) {
+        for (int e = P.qedge_ptr[p]; e < P.qedge_ptr[p + 1]; ++e)
+            if (P.qedge[e] == 0)
+                D.adj0 |= 1u << p;
+        for (int t = P.sym_ptr[p]; t < P.sym_ptr[p + 1]; ++t)
+            if (P.sym[t] == 0)
+                D.sym0 |= 1u << p;
+    }
     out->info = P;
     out->dev = D;
     return BEEP_OK;

@@ -1,7 +1,8 @@
 """Named query patterns, as .mtx-style directed edge lists (0-based, both
 directions listed, as README.md:55-64 of the reference shows for the
-triangle). Every pattern here has a central vertex adjacent to all others,
-which the reference requires (README.md:51-53)."""
+triangle). The patterns in NAMED have a central vertex adjacent to all
+others, which the reference requires (README.md:51-53); those in
+NON_CENTRAL do not and are counted by the library's list walker."""
 from __future__ import annotations
 
 import itertools
@@ -30,6 +31,28 @@ K5 = _undirected([(a, b) for a, b in itertools.combinations(range(5), 2)])
 CLAW = _undirected([(0, 1), (0, 2), (0, 3)])
 # Hub 0 plus a path on 2 vertices (a "wedge" with apex 0 is CLAW minus a leaf).
 WEDGE = _undirected([(0, 1), (0, 2)])
+
+# Queries without a central vertex.
+PATH4 = _undirected([(0, 1), (1, 2), (2, 3)])
+CYCLE4 = _undirected([(0, 1), (1, 2), (2, 3), (3, 0)])
+PATH5 = _undirected([(0, 1), (1, 2), (2, 3), (3, 4)])
+CYCLE5 = _undirected([(0, 1), (1, 2), (2, 3), (3, 4), (4, 0)])
+# Triangle 0-1-2 with pendants on 1 and 2.
+BULL = _undirected([(0, 1), (0, 2), (1, 2), (1, 3), (2, 4)])
+# 4-cycle 0-1-2-3 with a roof vertex 4 on the edge 0-1.
+HOUSE = _undirected([(0, 1), (1, 2), (2, 3), (3, 0), (0, 4), (1, 4)])
+# Complete bipartite K(2,3).
+K23 = _undirected([(a, b) for a in (0, 1) for b in (2, 3, 4)])
+
+NON_CENTRAL = {
+    "path4": PATH4,
+    "cycle4": CYCLE4,
+    "path5": PATH5,
+    "cycle5": CYCLE5,
+    "bull": BULL,
+    "house": HOUSE,
+    "k23": K23,
+}
 
 NAMED = {
     "triangle": TRIANGLE,

@@ -138,6 +138,10 @@ typedef struct beep_plan_info {
     int32_t aut_order;                                  /* |Aut(Q)| */
     int32_t restricted;    /* 1: every position is ordered after the root, so only the
                               root's higher-priority neighbours are searched */
+    int32_t central;       /* 1: position 0 is adjacent to every other position (the
+                              reference's requirement, README.md:51-53); 0: counted by the
+                              list-intersection walker (sgm, or sgc without an unmatched
+                              last position) */
 } beep_plan_info;
 beep_status beep_query_plan(const beep_query *q, beep_mode mode, beep_plan_info *out);
 
@@ -176,6 +180,10 @@ typedef struct beep_stats {
     uint64_t adjacency_bytes;   /* adjacency bytes the kernels must read (BEEP_OPT_ALG_BYTES) */
     uint64_t bitmap_bytes;      /* neighbourhood bitmap bytes of the large tier */
     uint64_t small_bytes, medium_bytes, large_bytes; /* adjacency_bytes by tier (BEEP_OPT_ALG_BYTES) */
+    int64_t roots_general;      /* roots of non-central queries (list walker) */
+    double general_ms;
+    int32_t general_launches;
+    int32_t pad0;
 } beep_stats;
 
 /* Count matches. Replaces SG_Match::run + count_subgraphs + final_counter

@@ -148,3 +148,27 @@ def test_oracle_matches_reference_binary(built, golden):
             assert rec["count"] == counts[mode], key
             checked += 1
     assert checked >= 15
+
+
+def test_non_central_golden_and_closed_forms(built):
+    """Brute-force counts of the queries without a central vertex: closed
+    forms on K_8 and the committed counts (tests/golden/non_central.json,
+    cross-checked with networkx when it was made) on the two smaller graphs."""
+    import json
+    import os
+
+    import beep_b200 as B
+
+    rp, col = csr_from_pairs(8, itertools.combinations(range(8), 2))
+    want = {"path4": 12 * math.comb(8, 4), "cycle4": 3 * math.comb(8, 4), "path5": 60 * math.comb(8, 5),
+            "cycle5": 12 * math.comb(8, 5), "k23": 10 * math.comb(8, 5)}
+    for name, w in want.items():
+        assert O.brute_force(rp, col, P.NON_CENTRAL[name]) == w, name
+    with open(os.path.join(os.path.dirname(__file__), "golden", "non_central.json")) as f:
+        gold = json.load(f)
+    gens = {"er": B.gen_erdos_renyi, "cl": B.gen_chung_lu, "rmat": B.gen_rmat}
+    for gname in ["er_60_p15_s3", "er_200_p05_s4"]:
+        rec = gold["graphs"][gname]
+        rp, col = gens[rec["kind"]](*rec["args"])
+        for pname, c in rec["counts"].items():
+            assert O.brute_force(rp, col, P.NON_CENTRAL[pname]) == c, (gname, pname)
