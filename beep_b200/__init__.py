@@ -122,6 +122,9 @@ class Stats(ctypes.Structure):
         ("general_ms", ctypes.c_double),
         ("general_launches", ctypes.c_int32),
         ("pad0", ctypes.c_int32),
+        ("alg_small_bytes", ctypes.c_uint64),
+        ("alg_medium_bytes", ctypes.c_uint64),
+        ("alg_large_bytes", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

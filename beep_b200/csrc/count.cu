@@ -595,8 +595,13 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
 // of one pair, packed as (pair << 32) | root. One launch per tier serves the
 // items of every pair of a call (the plain count is a call with one pair).
 // ---------------------------------------------------------------------------
+// Slots after the per-pair counters: adjacency bytes read per tier (3), the
+// algorithmic bytes of the searched roots per tier (3), 2 spare.
+constexpr uint32_t kAux = 8;
+
 struct PairDev {
     ViewDev v;
+    const uint32_t *g_rp, *g_col; // the graph's deduplicated input CSR (input ids)
     DevPlan pl;
     unsigned long long *count; // this pair's match count
     EnumDev en;                // enumeration output (out == nullptr: none)
@@ -1295,7 +1300,7 @@ __global__ void k_gather_dom(const PairDev *__restrict__ pairs, const uint64_t *
 // and split (12 B) plus its higher-priority list (4 B each).
 __global__ void k_alg_bytes(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ offs, uint32_t npairs,
                             const uint8_t *__restrict__ tier, uint64_t N, unsigned long long *bytes) {
-    unsigned long long acc[3] = {0, 0, 0};
+    unsigned long long acc[3] = {0, 0, 0}, alg[3] = {0, 0, 0};
     const int lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < N; t += warps) {
@@ -1313,13 +1318,28 @@ __global__ void k_alg_bytes(const PairDev *__restrict__ pairs, const uint64_t *_
             hd_range(pr.v, pr.asc, pr.v.col[beg + i], i, D, hb, he, xb, xe);
             a += 12ull + 4ull * (he - hb);
         }
-        acc[tc == 1 ? 0 : (tc == 4 ? 2 : 1)] += a;
+        // algorithmic bytes of building this root's neighbourhood bitmap from
+        // the input CSR: its list and each neighbour's full list, 4 bytes an
+        // entry, 4 * (deg r + sum over v in N(r) of deg v)
+        const uint32_t *grp = pairs[p].g_rp, *gcol = pairs[p].g_col;
+        const uint32_t u = pr.v.orig[(uint32_t)(t - offs[p])];
+        const uint32_t ub = grp[u], ue = grp[u + 1];
+        unsigned long long b = (lane == 0) ? 4ull * (ue - ub) : 0ull;
+        for (uint32_t k = ub + lane; k < ue; k += 32) {
+            const uint32_t w = gcol[k];
+            b += 4ull * (grp[w + 1] - grp[w]);
+        }
+        const int slot = tc == 1 ? 0 : (tc == 4 ? 2 : 1);
+        acc[slot] += a;
+        alg[slot] += b;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const unsigned long long x = warp_sum(acc[k]);
+        const unsigned long long x = warp_sum(acc[k]), y = warp_sum(alg[k]);
         if (lane == 0 && x)
             atomicAdd(&bytes[k], x);
+        if (lane == 0 && y)
+            atomicAdd(&bytes[3 + k], y);
     }
 }
 
@@ -1466,7 +1486,7 @@ struct LaunchPlan {
     unsigned long long *d_counts = nullptr; // np counts, np tuple counters, 4 byte counters
     unsigned *d_cursors = nullptr;
     uint32_t ncursors = 0;
-    unsigned long long *h_counts = nullptr; // pinned mirror (np + 4): the context's buffer, or owned when captured
+    unsigned long long *h_counts = nullptr; // pinned mirror (np + kAux): the context's buffer, or owned when captured
     bool own_h_counts = false;
     std::vector<LaunchRec> recs;
     bool enumerate = false;
@@ -1530,6 +1550,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         std::memset(&pd, 0, sizeof(pd));
         pd.v = ViewDev{v->row_ptr.as<uint32_t>(), v->col.as<uint32_t>(), v->split.as<uint32_t>(),
                        v->orig.as<uint32_t>()};
+        pd.g_rp = ps.g->row_ptr.as<uint32_t>();
+        pd.g_col = ps.g->col.as<uint32_t>();
         pd.pl = ps.plan.dev;
         pd.min_deg = (uint32_t)ps.plan.info.max_qdeg;
         pd.cap_deg = (options & BEEP_OPT_REFERENCE_ROOT_CAP)
@@ -1549,8 +1571,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     const uint32_t np = (uint32_t)hp.size();
     lp->np = np;
     tr.mark("views");
-    BEEP_TRY(ctx->host_results(np + 4, &lp->h_counts));
-    BEEP_TRY(lp->alloc(lp->d_counts, 2 * (size_t)np + 4));
+    BEEP_TRY(ctx->host_results(np + kAux, &lp->h_counts));
+    BEEP_TRY(lp->alloc(lp->d_counts, 2 * (size_t)np + kAux));
     lp->ncursors = 64;
     BEEP_TRY(lp->alloc(lp->d_cursors, lp->ncursors));
     if (np == 0) {
@@ -1899,7 +1921,7 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats
                   std::vector<double *> *sinks) {
     cudaStream_t s = ctx->stream;
     const uint32_t np = lp->np;
-    BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_counts, 0, (2 * (size_t)np + 4) * 8, s));
+    BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_counts, 0, (2 * (size_t)np + kAux) * 8, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_cursors, 0, lp->ncursors * 4, s));
     // The tiers are independent: large on the call's stream, medium and small
     // on two side streams forked from it and joined back at the end.
@@ -2003,7 +2025,7 @@ beep_status capture_plan(Ctx *ctx, LaunchPlan *lp) {
     // the captured read-back needs a host buffer that no other call reuses
     if (!lp->own_h_counts) {
         unsigned long long *h = nullptr;
-        BEEP_CUDA_TRY(cudaMallocHost(&h, (lp->np + 4) * sizeof(unsigned long long)));
+        BEEP_CUDA_TRY(cudaMallocHost(&h, (lp->np + kAux) * sizeof(unsigned long long)));
         lp->h_counts = h;
         lp->own_h_counts = true;
     }
@@ -2055,12 +2077,12 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
         cudaEventRecord(e1, s);
     if (lp->np > 0 && (options & BEEP_OPT_ALG_BYTES)) {
         unsigned long long *d_bytes = lp->d_counts + 2 * (size_t)lp->np;
-        BEEP_CUDA_TRY(cudaMemsetAsync(d_bytes, 0, 32, s));
+        BEEP_CUDA_TRY(cudaMemsetAsync(d_bytes, 0, kAux * 8, s));
         const int gv = std::max(1, (int)std::min<uint64_t>((lp->N + 255) / 256, (uint64_t)ctx->num_sms * 32));
         k_alg_bytes<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, lp->np, lp->d_tier, lp->N, d_bytes);
         BEEP_CUDA_TRY(cudaGetLastError());
         st.kernel_launches += 1;
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts + lp->np, d_bytes, 32, cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts + lp->np, d_bytes, kAux * 8, cudaMemcpyDeviceToHost, s));
     }
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     if (timing) {
@@ -2097,6 +2119,9 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
         st.medium_bytes = lp->h_counts[lp->np + 1];
         st.large_bytes = lp->h_counts[lp->np + 2];
         st.adjacency_bytes = st.small_bytes + st.medium_bytes + st.large_bytes;
+        st.alg_small_bytes = lp->h_counts[lp->np + 3];
+        st.alg_medium_bytes = lp->h_counts[lp->np + 4];
+        st.alg_large_bytes = lp->h_counts[lp->np + 5];
     }
     if (stats)
         *stats = st;
@@ -2106,7 +2131,7 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
 beep_status launch_plan_async(Ctx *ctx, LaunchPlan *lp) {
     if (!lp->own_h_counts) {
         unsigned long long *h = nullptr;
-        BEEP_CUDA_TRY(cudaMallocHost(&h, (lp->np + 4) * sizeof(unsigned long long)));
+        BEEP_CUDA_TRY(cudaMallocHost(&h, (lp->np + kAux) * sizeof(unsigned long long)));
         lp->h_counts = h;
         lp->own_h_counts = true;
     }

@@ -184,6 +184,11 @@ typedef struct beep_stats {
     double general_ms;
     int32_t general_launches;
     int32_t pad0;
+    /* BEEP_OPT_ALG_BYTES: algorithmic bytes of the searched roots by tier,
+     * 4 * (deg r + sum of deg v over v in N(r)) on the input CSR -- the
+     * adjacency traffic of building each root's neighbourhood bitmap from the
+     * CSR, whatever the kernels actually read */
+    uint64_t alg_small_bytes, alg_medium_bytes, alg_large_bytes;
 } beep_stats;
 
 /* Count matches. Replaces SG_Match::run + count_subgraphs + final_counter
