@@ -187,6 +187,8 @@ _SIGNATURES = [
                                          _P(ctypes.c_int32)]),
     ("beep_write_bel", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_int32)]),
     ("beep_convert", ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, _P(ctypes.c_uint64)]),
+    ("beep_batch_autotune", ctypes.c_int, [_vp, ctypes.c_uint32, _P(ctypes.c_uint32 * 4), _P(ctypes.c_double)]),
+    ("beep_batch_set_tiers", ctypes.c_int, [_vp, _P(ctypes.c_uint32 * 4)]),
 ]
 
 
@@ -440,6 +442,20 @@ class Batch:
         _check(lib().beep_batch_run(self._h, int(options), counts, ctypes.byref(st)))
         out = [int(counts[i]) for i in range(n)]
         return (out, st.as_dict()) if stats else out
+
+    TIER_KEYS = ("tiny_max", "small_max", "med_a_max", "med_max")
+
+    def autotune(self, options: int = 0) -> dict:
+        """Pick the tier limits by measurement (beep_batch_autotune); returns
+        them with the best counting time in ms."""
+        cfg = (ctypes.c_uint32 * 4)()
+        ms = ctypes.c_double()
+        _check(lib().beep_batch_autotune(self._h, int(options), ctypes.byref(cfg), ctypes.byref(ms)))
+        return {**dict(zip(self.TIER_KEYS, list(cfg))), "count_ms": ms.value}
+
+    def set_tiers(self, tiers: dict) -> None:
+        cfg = (ctypes.c_uint32 * 4)(*[int(tiers[k]) for k in self.TIER_KEYS])
+        _check(lib().beep_batch_set_tiers(self._h, ctypes.byref(cfg)))
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -452,6 +452,7 @@ struct beep_batch {
     std::vector<beep::PairSpec> specs;
     beep::LaunchPlanPtr plan;
     uint32_t planned_options = 0;
+    beep::TierCfg tiers;
 };
 
 beep_status beep_batch_create(beep_ctx *ctx, beep_batch **out) {
@@ -501,7 +502,7 @@ beep_status beep_batch_run(beep_batch *b, uint32_t options, uint64_t *counts, be
         cudaEventCreate(&p0);
         cudaEventCreate(&p1);
         cudaEventRecord(p0, ctx->stream);
-        BEEP_TRY(plan_pairs(ctx, b->specs, plan_opts, &b->plan));
+        BEEP_TRY(plan_pairs(ctx, b->specs, plan_opts, &b->plan, b->tiers));
         b->planned_options = plan_opts;
         cudaEventRecord(p1, ctx->stream);
         cudaEventSynchronize(p1);
@@ -519,6 +520,60 @@ beep_status beep_batch_run(beep_batch *b, uint32_t options, uint64_t *counts, be
     ctx->launches += (uint64_t)st.kernel_launches;
     if (stats)
         *stats = st;
+    return BEEP_OK;
+}
+
+beep_status beep_batch_set_tiers(beep_batch *b, const beep_tier_cfg *cfg) {
+    if (!b || !cfg)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_batch_set_tiers: bad arguments");
+    BEEP_TRY(bind(b->ctx));
+    cudaStreamSynchronize(b->ctx->impl.stream);
+    b->tiers = TierCfg{cfg->tiny_max, cfg->small_max, cfg->med_a_max, cfg->med_max};
+    b->plan.reset(); // the next run plans (and captures) with the new limits
+    return BEEP_OK;
+}
+
+beep_status beep_batch_autotune(beep_batch *b, uint32_t options, beep_tier_cfg *chosen, double *best_count_ms) {
+    if (!b)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_batch_autotune: bad arguments");
+    BEEP_TRY(bind(b->ctx));
+    Ctx *ctx = &b->ctx->impl;
+    const uint32_t plan_opts = options & BEEP_OPT_REFERENCE_ROOT_CAP;
+    std::vector<uint64_t> counts(std::max<size_t>(b->specs.size(), 1));
+    auto measure = [&](const TierCfg &cfg, double *ms) -> beep_status {
+        LaunchPlanPtr lp;
+        BEEP_TRY(plan_pairs(ctx, b->specs, plan_opts, &lp, cfg));
+        beep_stats st;
+        BEEP_TRY(execute_plan(ctx, lp.get(), BEEP_OPT_TIMING, &b->specs, counts.data(), b->specs.size(), &st));
+        ctx->launches += (uint64_t)st.kernel_launches;
+        *ms = st.count_ms;
+        return BEEP_OK;
+    };
+    TierCfg best = b->tiers;
+    double best_ms = 0;
+    BEEP_TRY(measure(best, &best_ms)); // also builds the views, so later candidates time only the counting
+    BEEP_TRY(measure(best, &best_ms));
+    const std::vector<uint32_t> cand[4] = {{0, 8, 16}, {32, 64}, {128, 256}, {512, 1024}};
+    for (int k = 0; k < 4; ++k)
+        for (uint32_t val : cand[k]) {
+            TierCfg c = best;
+            uint32_t *f[4] = {&c.tiny_max, &c.small_max, &c.med_a_max, &c.med_max};
+            if (*f[k] == val)
+                continue;
+            *f[k] = val;
+            double ms = 0;
+            BEEP_TRY(measure(c, &ms));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+    b->tiers = best;
+    b->plan.reset();
+    if (chosen)
+        *chosen = beep_tier_cfg{best.tiny_max, best.small_max, best.med_a_max, best.med_max};
+    if (best_count_ms)
+        *best_count_ms = best_ms;
     return BEEP_OK;
 }
 

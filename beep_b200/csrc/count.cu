@@ -1205,8 +1205,8 @@ __device__ __forceinline__ uint32_t find_pair(const uint64_t *__restrict__ offs,
 // tier[t] for flattened vertex t; dom[t] = its domain size; per tier the
 // largest domain and per (tier, depth) the number of roots.
 __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ offs, uint32_t npairs,
-                           uint64_t N, uint8_t *tier, uint32_t *dom, unsigned *tier_max, unsigned *tier_depth,
-                           unsigned *tiny_depth) {
+                           uint64_t N, TierCfg cfg, uint8_t *tier, uint32_t *dom, unsigned *tier_max,
+                           unsigned *tier_depth, unsigned *tiny_depth) {
     __shared__ unsigned s_hist[kTiers * kDepths];
     __shared__ unsigned s_tiny[kDepths];
     for (int i = threadIdx.x; i < kTiers * kDepths; i += blockDim.x)
@@ -1241,14 +1241,14 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
                 D -= j0; // level-1 tasks of the list walker
             }
         } else if (root_ok && D + 1 >= (uint32_t)pd.pl.dend) {
-            tc = D <= kSmallMaxD ? 1 : (D <= kMediumAMaxD ? 2 : (D <= kMediumMaxD ? 3 : 4));
+            tc = D <= cfg.small_max ? 1 : (D <= cfg.med_a_max ? 2 : (D <= cfg.med_max ? 3 : 4));
         }
         tier[t] = tc;
         dom[t] = D;
         if (tc) {
             mx[tc - 1] = max(mx[tc - 1], D);
             atomicAdd(&s_hist[(tc - 1) * kDepths + pd.pl.dend], 1u);
-            if (tc == 1 && D <= (uint32_t)kTinyMaxD)
+            if (tc == 1 && D <= cfg.tiny_max)
                 atomicAdd(&s_tiny[pd.pl.dend], 1u);
         }
     }
@@ -1516,7 +1516,8 @@ struct LaunchPlan {
 
 void LaunchPlanDeleter::operator()(LaunchPlan *p) const { delete p; }
 
-beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out) {
+beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out,
+                       const TierCfg &tiers) {
     cudaStream_t s = ctx->stream;
     PhaseTrace tr("plan", s);
     LaunchPlanPtr lp(new LaunchPlan);
@@ -1607,7 +1608,12 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     // per (tier, depth), [64, 64 + kDepths) tiny small-tier roots per depth,
     // [80] selection count
     static_assert(8 + kTiers * kDepths <= 64, "d_misc layout");
-    k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, lp->d_tier, d_dom, d_misc, d_misc + 8,
+    TierCfg cfg = tiers;
+    cfg.tiny_max = std::min<uint32_t>(cfg.tiny_max, kTinyMaxD);
+    cfg.small_max = std::min<uint32_t>(cfg.small_max, kSmallMaxD);
+    cfg.med_a_max = std::min<uint32_t>(cfg.med_a_max, kMediumAMaxD);
+    cfg.med_max = std::min<uint32_t>(cfg.med_max, kMediumMaxD);
+    k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, cfg, lp->d_tier, d_dom, d_misc, d_misc + 8,
                                   d_misc + 64);
     BEEP_CUDA_TRY(cudaGetLastError());
     st.kernel_launches += 1;

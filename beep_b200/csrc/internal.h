@@ -289,7 +289,15 @@ struct LaunchPlanDeleter {
     void operator()(LaunchPlan *p) const;
 };
 using LaunchPlanPtr = std::unique_ptr<LaunchPlan, LaunchPlanDeleter>;
-beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out);
+// Domain-size limits of the kernel tiers (each at most the compile-time
+// bound of its kernel): 8-lane small groups up to tiny_max, warp groups up to
+// small_max (<= 64), thread-walker blocks up to med_a_max (<= 256), warp-walker
+// blocks up to med_max (<= 1024), the global-arena tier above.
+struct TierCfg {
+    uint32_t tiny_max = 16, small_max = 64, med_a_max = 256, med_max = 1024;
+};
+beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out,
+                       const TierCfg &tiers = TierCfg());
 // Capture the plan's launches into a CUDA graph (relaunched by execute_plan).
 beep_status capture_plan(Ctx *ctx, LaunchPlan *lp);
 beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::vector<PairSpec> *specs,

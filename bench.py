@@ -345,6 +345,11 @@ def bench_batched(args):
     batch = B.Batch(ctx)
     for g, q in pairs:
         batch.add(g, q)
+    tuned = None
+    if not args.c4_no_autotune:
+        t0 = time.perf_counter()
+        tuned = batch.autotune()  # tier limits by measurement, before the timed replays
+        tuned["seconds"] = time.perf_counter() - t0
     t0 = time.perf_counter()
     first = batch.run()  # plans and captures
     plan_s = time.perf_counter() - t0
@@ -368,7 +373,7 @@ def bench_batched(args):
             "plain_loop": {"value": plain_total / plain_s, "ms": plain_s * 1e3,
                            "what": "beep_count per pair, same pairs, views resident"},
             "speedup_vs_plain_loop": plain_s / step_s, "plan_and_capture_ms": plan_s * 1e3,
-            "generate_s": gen_s}
+            "autotuned_tiers": tuned, "generate_s": gen_s}
     print(json.dumps(line), flush=True)
     batch.close()
     for g in graphs:
@@ -466,6 +471,7 @@ def main():
     ap.add_argument("--c4-graphs", type=int, default=256)
     ap.add_argument("--c4-max-scale", type=float, default=18.0)
     ap.add_argument("--c4-max-degree", type=float, default=64.0)
+    ap.add_argument("--c4-no-autotune", action="store_true")
     ap.add_argument("--c5-graphs", type=int, default=32)
     ap.add_argument("--c5-max-log10-edges", type=float, default=7.0)
     ap.add_argument("--c5-rate", type=float, default=2000.0)

@@ -230,6 +230,14 @@ enum {
     /* Run the planned launches directly instead of through the CUDA graph. */
     BEEP_OPT_NO_GRAPH = 1u << 4
 };
+/* Domain-size limits of the kernel tiers a batch plans with (each clamped to
+ * its kernel's bound: 16, 64, 256, 1024). A root whose search domain has D
+ * vertices goes to 8-lane groups if D <= tiny_max, warp groups if
+ * D <= small_max, thread-walker blocks if D <= med_a_max, warp-walker blocks if
+ * D <= med_max, and the global-arena tier above. */
+typedef struct beep_tier_cfg {
+    uint32_t tiny_max, small_max, med_a_max, med_max;
+} beep_tier_cfg;
 beep_status beep_batch_create(beep_ctx *ctx, beep_batch **out);
 beep_status beep_batch_add(beep_batch *b, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t *index);
 /* counts[i] receives the count of the i-th added pair (array of at least
@@ -237,6 +245,14 @@ beep_status beep_batch_add(beep_batch *b, beep_graph *g, const beep_query *q, be
 beep_status beep_batch_run(beep_batch *b, uint32_t options, uint64_t *counts, beep_stats *stats);
 beep_status beep_batch_size(const beep_batch *b, uint32_t *out);
 beep_status beep_batch_destroy(beep_batch *b);
+/* Pick the batch's tier limits by measurement: coordinate descent over
+ * tiny_max {0, 8, 16}, small_max {32, 64}, med_a_max {128, 256} and
+ * med_max {512, 1024}, each candidate planned and run once (no CUDA graph)
+ * with its counting kernels timed by CUDA events; later runs plan with the
+ * fastest. Counts do not depend on the limits. chosen and best_count_ms may be
+ * NULL. */
+beep_status beep_batch_autotune(beep_batch *b, uint32_t options, beep_tier_cfg *chosen, double *best_count_ms);
+beep_status beep_batch_set_tiers(beep_batch *b, const beep_tier_cfg *cfg);
 
 /* ---- serving ------------------------------------------------------------ */
 

@@ -80,3 +80,27 @@ def test_batch_mixed_depths_and_large_roots(ctx):
     batch.close()
     g1.close()
     g2.close()
+
+
+def test_tier_limits_and_autotune_keep_counts(ctx):
+    """Counts do not depend on which tier a root runs in: every limit set the
+    autotuner can pick, and the one it picks, give the same counts."""
+    gs = [(rp, col, B.Graph.from_csr(ctx, rp, col)) for rp, col in graphs()[:3]]
+    pats = [P.TRIANGLE, P.DIAMOND, P.K4, P.W5, P.NAMED["tailed_triangle"]]
+    batch = B.Batch(ctx)
+    for _, _, g in gs:
+        for q in pats:
+            batch.add(g, q, B.SGM)
+    base = batch.run()
+    for tiers in [dict(tiny_max=0, small_max=32, med_a_max=128, med_max=512),
+                  dict(tiny_max=8, small_max=64, med_a_max=256, med_max=512),
+                  dict(tiny_max=16, small_max=32, med_a_max=256, med_max=1024)]:
+        batch.set_tiers(tiers)
+        assert batch.run() == base, tiers
+    best = batch.autotune()
+    assert best["small_max"] in (32, 64) and best["count_ms"] > 0
+    assert batch.run() == base
+    assert batch.run(B.OPT_NO_GRAPH) == base
+    batch.close()
+    for _, _, g in gs:
+        g.close()
