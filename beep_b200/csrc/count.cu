@@ -32,6 +32,7 @@
 #include <mutex>
 
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "internal.h"
 
@@ -1406,45 +1407,6 @@ beep_status launch_large_dfs(int dend, int grid, cudaStream_t s, const PairDev *
     return BEEP_OK;
 }
 
-struct Timer {
-    struct Rec {
-        cudaEvent_t a, b;
-        double *out;
-    };
-    bool on = false;
-    cudaStream_t s = nullptr;
-    std::vector<Rec> recs;
-    int start() {
-        if (!on)
-            return -1;
-        Rec r{nullptr, nullptr, nullptr};
-        cudaEventCreate(&r.a);
-        cudaEventCreate(&r.b);
-        cudaEventRecord(r.a, s);
-        recs.push_back(r);
-        return (int)recs.size() - 1;
-    }
-    void stop(int id, double *out) {
-        if (id < 0)
-            return;
-        cudaEventRecord(recs[id].b, s);
-        recs[id].out = out;
-    }
-    void collect() {
-        for (auto &r : recs) {
-            float ms = 0;
-            if (r.out) {
-                cudaEventSynchronize(r.b);
-                cudaEventElapsedTime(&ms, r.a, r.b);
-                *r.out += ms;
-            }
-            cudaEventDestroy(r.a);
-            cudaEventDestroy(r.b);
-        }
-        recs.clear();
-    }
-    ~Timer() { collect(); }
-};
 
 } // namespace
 
@@ -1643,7 +1605,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         const uint32_t n_k = tier_n[k];
         BEEP_TRY(lp->alloc(list, n_k));
         size_t tb = 0;
-        cub::CountingInputIterator<uint32_t> it(0);
+        thrust::counting_iterator<uint32_t> it(0);
         TierSel sel{lp->d_tier, (uint8_t)(k + 1)};
         unsigned *d_ns = d_misc + 80;
         BEEP_CUDA_TRY(cub::DeviceSelect::If(nullptr, tb, it, d_sel, d_ns, N, sel, s));
