@@ -335,8 +335,12 @@ __global__ void k_fill_key_chunks(const uint32_t *__restrict__ col, const uint32
     }
 }
 
-__global__ void k_keys_low(const uint64_t *__restrict__ keys, int64_t m, int rb, uint32_t *col) {
+// The first *m_live sorted keys are the view's entries (the dropped ones,
+// all ones, sort last).
+__global__ void k_keys_low(const uint64_t *__restrict__ keys, const uint32_t *__restrict__ m_live, int rb,
+                           uint32_t *col) {
     const uint64_t mask = ((uint64_t)1 << rb) - 1;
+    const int64_t m = *m_live;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
         col[i] = (uint32_t)(keys[i] & mask);
 }
@@ -660,18 +664,15 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, new_deg, nrp, na + 1, s));
     BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
     BEEP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ctx->scratch.ptr, tb, new_deg, nrp, na + 1, s));
-    uint32_t *h2 = reinterpret_cast<uint32_t *>(ctx->h_pinned);
-    BEEP_CUDA_TRY(cudaMemcpyAsync(h2, nrp + na, 4, cudaMemcpyDeviceToHost, s));
-    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
-    const uint32_t h_m = h2[0];
-    v->m = h_m;
+    // The view's entry count nrp[na] stays on the device: the buffers are
+    // sized for all m input entries and the kernels read the count there.
     tr.mark("rank_scan");
-    BEEP_TRY(ctx->grow(v->col, (size_t)(h_m > 0 ? h_m : 1) * 4));
+    BEEP_TRY(ctx->grow(v->col, (size_t)(m > 0 ? m : 1) * 4));
     // rank bits: every rank is below na < 2^rb
     int rb = 1;
     while (rb < 32 && ((uint64_t)1 << rb) <= (uint64_t)na)
         ++rb;
-    if (h_m > 0) {
+    if (m > 0 && na > 0) {
         BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks, 0, 4, s));
         k_fill_keys<<<gv, 256, 0, s>>>(rp, col, rank, n, rb, ekeys, chunks, d_nchunks, ucap);
         k_fill_key_chunks<<<ctx->num_sms * 8, 256, 0, s>>>(col, rank, chunks, d_nchunks, ucap, rb, ekeys);
@@ -679,12 +680,12 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
         BEEP_CUDA_TRY(cudaGetLastError());
     }
     tr.mark("fill");
-    if (h_m > 0) {
+    if (m > 0 && na > 0) {
         tb = 0;
         BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, ekeys, ekeys2, m, 0, 2 * rb, s));
         BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
         BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(ctx->scratch.ptr, tb, ekeys, ekeys2, m, 0, 2 * rb, s));
-        k_keys_low<<<grid_for(h_m, 256, ctx->num_sms), 256, 0, s>>>(ekeys2, h_m, rb, v->col.as<uint32_t>());
+        k_keys_low<<<grid_for(m, 256, ctx->num_sms), 256, 0, s>>>(ekeys2, nrp + na, rb, v->col.as<uint32_t>());
         ++ctx->launches;
         BEEP_CUDA_TRY(cudaGetLastError());
     }

@@ -166,10 +166,9 @@ struct View {
     int32_t min_qdeg = 0;
     int32_t asc = 1;
     int64_t n = 0;           // vertices with degree > 0 after peeling
-    int64_t m = 0;           // directed edges
     int32_t peel_rounds = 0;
     DevBuf row_ptr;          // u32[n+1]
-    DevBuf col;              // u32[m], new ids, rows ascending
+    DevBuf col;              // u32[row_ptr[n]] (sized for the graph's m), new ids, rows ascending
     DevBuf orig;             // u32[n]: new id -> input id
     DevBuf split;            // u32[n]: neighbours with a smaller new id
 };
