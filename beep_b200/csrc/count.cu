@@ -1271,18 +1271,36 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
             atomicAdd(&tiny_depth[i], s_tiny[i]);
 }
 
-// Selected flattened indices -> items and sort keys: depth, then (by_domain 1,
-// medium) largest domain first or (by_domain 2, small) smallest first.
-__global__ void k_make_items(const uint32_t *__restrict__ sel, uint32_t ns, const PairDev *__restrict__ pairs,
-                             const uint64_t *__restrict__ offs, uint32_t npairs, const uint32_t *__restrict__ dom,
-                             int by_domain, uint64_t *items, uint32_t *keys) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
-        const uint32_t t = sel[i];
+// Sort keys of every flattened vertex for all item lists at once:
+// (tier, depth, domain order) -- small roots by domain ascending, medium and
+// large ones by domain descending (heaviest first), list-walker roots by
+// depth only; non-roots last.
+__global__ void k_list_keys(const uint8_t *__restrict__ tier, const uint32_t *__restrict__ dom,
+                            const PairDev *__restrict__ pairs, const uint64_t *__restrict__ offs, uint32_t npairs,
+                            uint64_t N, uint32_t *keys, uint32_t *vals) {
+    constexpr uint32_t kDomMask = (1u << 24) - 1u;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t tc = tier[t];
+        uint32_t key = 0xffffffffu;
+        if (tc) {
+            const uint32_t p = find_pair(offs, npairs, t);
+            const uint32_t dend = (uint32_t)pairs[p].pl.dend;
+            const uint32_t d = min(dom[t], kDomMask);
+            const uint32_t dk = tc == 1 ? d : (tc == 5 ? 0u : kDomMask - d);
+            key = ((tc - 1) << 28) | (dend << 24) | dk;
+        }
+        keys[t] = key;
+        vals[t] = (uint32_t)t;
+    }
+}
+
+// Sorted flattened indices of the roots -> items (pair << 32 | root).
+__global__ void k_make_items(const uint32_t *__restrict__ sorted, uint32_t n, const uint64_t *__restrict__ offs,
+                             uint32_t npairs, uint64_t *items) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t t = sorted[i];
         const uint32_t p = find_pair(offs, npairs, t);
         items[i] = ((uint64_t)p << 32) | (uint64_t)(t - offs[p]);
-        const uint32_t dend = (uint32_t)pairs[p].pl.dend;
-        const uint32_t d = min(dom[t], 65535u);
-        keys[i] = by_domain == 1 ? (dend << 16) | (65535u - d) : (by_domain == 2 ? (dend << 16) | d : dend);
     }
 }
 
@@ -1347,11 +1365,6 @@ __global__ void k_alg_bytes(const PairDev *__restrict__ pairs, const uint64_t *_
     }
 }
 
-struct TierSel {
-    const uint8_t *tier;
-    uint8_t want;
-    __host__ __device__ bool operator()(const uint32_t &i) const { return tier[i] == want; }
-};
 
 // ---------------------------------------------------------------------------
 // launch helpers (one instantiation per depth)
@@ -1558,13 +1571,11 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     BEEP_TRY(lp->alloc(lp->d_tier, N));
     uint32_t *d_dom, *d_sel, *d_keys, *d_keys2;
     unsigned *d_misc;
-    uint64_t *d_tmp_items;
     BEEP_TRY(lp->alloc(d_dom, N));
     BEEP_TRY(lp->alloc(d_sel, N));
     BEEP_TRY(lp->alloc(d_keys, N));
     BEEP_TRY(lp->alloc(d_keys2, N));
     BEEP_TRY(lp->alloc(d_misc, 256));
-    BEEP_TRY(lp->alloc(d_tmp_items, N));
     BEEP_CUDA_TRY(cudaMemcpyAsync(lp->d_pairs, hp.data(), np * sizeof(PairDev), cudaMemcpyHostToDevice, s));
     BEEP_CUDA_TRY(cudaMemcpyAsync(lp->d_offs, offs.data(), (np + 1) * 8, cudaMemcpyHostToDevice, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(d_misc, 0, 256 * 4, s));
@@ -1603,35 +1614,28 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     uint32_t next_cursor = 0;
     auto cursor = [&]() -> unsigned * { return lp->d_cursors + (next_cursor++ % lp->ncursors); };
 
-    // item list of tier k in its own buffer, sorted by depth (medium: largest domain first)
-    auto make_list = [&](int k, uint64_t *&list) -> beep_status {
-        const uint32_t n_k = tier_n[k];
-        BEEP_TRY(lp->alloc(list, n_k));
-        size_t tb = 0;
-        thrust::counting_iterator<uint32_t> it(0);
-        TierSel sel{lp->d_tier, (uint8_t)(k + 1)};
-        unsigned *d_ns = d_misc + 80;
-        BEEP_CUDA_TRY(cub::DeviceSelect::If(nullptr, tb, it, d_sel, d_ns, N, sel, s));
-        BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
-        BEEP_CUDA_TRY(cub::DeviceSelect::If(ctx->scratch.ptr, tb, it, d_sel, d_ns, N, sel, s));
-        const int by_domain = (k == 1 || k == 2) ? 1 : (k == 0 ? 2 : 0);
-        int depths = 0;
-        for (int d = 0; d < kDepths; ++d)
-            depths += tier_depth[k * kDepths + d] > 0;
-        const bool sort = depths > 1 || by_domain;
-        k_make_items<<<std::max(1u, std::min(n_k / 256 + 1, 4096u)), 256, 0, s>>>(
-            d_sel, n_k, lp->d_pairs, lp->d_offs, np, d_dom, by_domain, sort ? d_tmp_items : list, d_keys);
+    // All item lists by one sort of (tier, depth, domain order) keys over the
+    // flattened vertices; tier k's list is a contiguous run of the result.
+    uint64_t *all_items = nullptr;
+    uint32_t list_off[kTiers + 1] = {0};
+    for (int k = 0; k < kTiers; ++k)
+        list_off[k + 1] = list_off[k] + tier_n[k];
+    BEEP_TRY(lp->alloc(all_items, list_off[kTiers]));
+    if (list_off[kTiers] > 0) {
+        k_list_keys<<<gv, 256, 0, s>>>(lp->d_tier, d_dom, lp->d_pairs, lp->d_offs, np, N, d_keys, d_sel);
         BEEP_CUDA_TRY(cudaGetLastError());
-        st.kernel_launches += 1;
-        if (sort) {
-            tb = 0;
-            const int end_bit = by_domain ? 20 : 4;
-            BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_keys, d_keys2, d_tmp_items, list, n_k, 0,
-                                                          end_bit, s));
-            BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
-            BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ctx->scratch.ptr, tb, d_keys, d_keys2, d_tmp_items, list,
-                                                          n_k, 0, end_bit, s));
-        }
+        size_t tb = 0;
+        BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_keys, d_keys2, d_sel, d_dom, N, 0, 31, s));
+        BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
+        BEEP_CUDA_TRY(
+            cub::DeviceRadixSort::SortPairs(ctx->scratch.ptr, tb, d_keys, d_keys2, d_sel, d_dom, N, 0, 31, s));
+        k_make_items<<<std::max(1u, std::min(list_off[kTiers] / 256 + 1, 4096u)), 256, 0, s>>>(
+            d_dom, list_off[kTiers], lp->d_offs, np, all_items);
+        BEEP_CUDA_TRY(cudaGetLastError());
+        st.kernel_launches += 2;
+    }
+    auto make_list = [&](int k, uint64_t *&list) -> beep_status {
+        list = all_items + list_off[k];
         return BEEP_OK;
     };
 
