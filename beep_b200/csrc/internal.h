@@ -293,7 +293,7 @@ using LaunchPlanPtr = std::unique_ptr<LaunchPlan, LaunchPlanDeleter>;
 // small_max (<= 64), thread-walker blocks up to med_a_max (<= 256), warp-walker
 // blocks up to med_max (<= 1024), the global-arena tier above.
 struct TierCfg {
-    uint32_t tiny_max = 16, small_max = 64, med_a_max = 256, med_max = 1024;
+    uint32_t tiny_max = 8, small_max = 64, med_a_max = 256, med_max = 1024; // tiny_max 8: the tuner's pick on C2
 };
 beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out,
                        const TierCfg &tiers = TierCfg());

@@ -231,7 +231,7 @@ enum {
     BEEP_OPT_NO_GRAPH = 1u << 4
 };
 /* Domain-size limits of the kernel tiers a batch plans with (each clamped to
- * its kernel's bound: 16, 64, 256, 1024). A root whose search domain has D
+ * its kernel's bound: 16, 64, 256, 1024; defaults 8, 64, 256, 1024). A root whose search domain has D
  * vertices goes to 8-lane groups if D <= tiny_max, warp groups if
  * D <= small_max, thread-walker blocks if D <= med_a_max, warp-walker blocks if
  * D <= med_max, and the global-arena tier above. */
