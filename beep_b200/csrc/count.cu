@@ -1002,7 +1002,8 @@ template <int DEND, bool ENUM>
 __global__ void __launch_bounds__(256) k_large_dfs(const PairDev *__restrict__ pairs, Batch bt,
                                                    const uint32_t *arena, unsigned *cursor) {
     const int lane = threadIdx.x & 31;
-    const uint32_t total = bt.tstart[bt.nb];
+    const uint32_t base0 = bt.tstart[0]; // the items' tasks are tstart[0] .. tstart[nb] - 1
+    const uint32_t total = bt.tstart[bt.nb] - base0;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
     EnumCtx ec;
@@ -1014,6 +1015,7 @@ __global__ void __launch_bounds__(256) k_large_dfs(const PairDev *__restrict__ p
         t = __shfl_sync(kFull, t, 0);
         if (t >= total)
             break;
+        t += base0;
         const uint32_t b = find_batch(bt.tstart, bt.nb, t);
         const uint64_t it = bt.item[b];
         const uint32_t p = item_pair(it), r = item_root(it);
@@ -1211,7 +1213,7 @@ __device__ __forceinline__ uint32_t find_pair(const uint64_t *__restrict__ offs,
 // largest domain and per (tier, depth) the number of roots.
 __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ offs, uint32_t npairs,
                            uint64_t N, TierCfg cfg, uint8_t *tier, uint32_t *dom, unsigned *tier_max,
-                           unsigned *tier_depth, unsigned *tiny_depth) {
+                           unsigned *tier_depth, unsigned *tiny_depth, unsigned long long *large_words) {
     __shared__ unsigned s_hist[kTiers * kDepths];
     __shared__ unsigned s_tiny[kDepths];
     for (int i = threadIdx.x; i < kTiers * kDepths; i += blockDim.x)
@@ -1250,6 +1252,10 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
         }
         tier[t] = tc;
         dom[t] = D;
+        if (tc == 4) {
+            const uint32_t rn = pd.pl.rows_needed, rlo = rn == 2 ? 0u : (rn == 1 ? j0 : D);
+            atomicAdd(large_words, ((uint64_t)(D - rlo) * ((D + 31) / 32) + 31) & ~(uint64_t)31);
+        }
         if (tc) {
             mx[tc - 1] = max(mx[tc - 1], D);
             atomicAdd(&s_hist[(tc - 1) * kDepths + pd.pl.dend], 1u);
@@ -1302,6 +1308,21 @@ __global__ void k_make_items(const uint32_t *__restrict__ sorted, uint32_t n, co
         const uint32_t t = sorted[i];
         const uint32_t p = find_pair(offs, npairs, t);
         items[i] = ((uint64_t)p << 32) | (uint64_t)(t - offs[p]);
+    }
+}
+
+// Arena words, row chunks and level-1 tasks of each listed large root
+// (D, j0 from k_gather_dom).
+__global__ void k_large_meta(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ items, uint32_t nl,
+                             const uint32_t *__restrict__ D_in, const uint32_t *__restrict__ j0_in,
+                             unsigned long long *words, uint32_t *chunks, uint32_t *tasks) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nl; i += gridDim.x * blockDim.x) {
+        const uint32_t D = D_in[i], j0 = j0_in[i];
+        const uint32_t rn = (uint32_t)pairs[item_pair(items[i])].pl.rows_needed;
+        const uint32_t rlo = rn == 2 ? 0u : (rn == 1 ? j0 : D);
+        words[i] = ((unsigned long long)(D - rlo) * ((D + 31) / 32) + 31) & ~31ull;
+        chunks[i] = (D + kRowsPerChunk - 1) / kRowsPerChunk;
+        tasks[i] = D - j0;
     }
 }
 
@@ -1583,7 +1604,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     const int gv = std::max(1, (int)std::min<uint64_t>((N + 255) / 256, (uint64_t)ctx->num_sms * 32));
     // d_misc: [0, 8) largest domain per tier, [8, 8 + kTiers * kDepths) roots
     // per (tier, depth), [64, 64 + kDepths) tiny small-tier roots per depth,
-    // [80] selection count
+    // [84, 86) arena words of the large tier (u64)
     static_assert(8 + kTiers * kDepths <= 64, "d_misc layout");
     TierCfg cfg = tiers;
     cfg.tiny_max = std::min<uint32_t>(cfg.tiny_max, kTinyMaxD);
@@ -1591,15 +1612,17 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     cfg.med_a_max = std::min<uint32_t>(cfg.med_a_max, kMediumAMaxD);
     cfg.med_max = std::min<uint32_t>(cfg.med_max, kMediumMaxD);
     k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, cfg, lp->d_tier, d_dom, d_misc, d_misc + 8,
-                                  d_misc + 64);
+                                  d_misc + 64, reinterpret_cast<unsigned long long *>(d_misc + 84));
     BEEP_CUDA_TRY(cudaGetLastError());
     st.kernel_launches += 1;
-    unsigned h_misc[80];
+    unsigned h_misc[88];
     BEEP_CUDA_TRY(cudaMemcpyAsync(h_misc, d_misc, sizeof(h_misc), cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     const unsigned *tier_max = h_misc;
     const unsigned *tier_depth = h_misc + 8;
     const unsigned *tiny_depth = h_misc + 64;
+    uint64_t large_words = 0;
+    std::memcpy(&large_words, h_misc + 84, 8);
     uint32_t tier_n[kTiers];
     for (int k = 0; k < kTiers; ++k) {
         tier_n[k] = 0;
@@ -1640,8 +1663,85 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         return BEEP_OK;
     };
 
-    // large tier: batches of roots whose bitmaps fit the arena
+    // large tier, one batch planned on the device when every root's bitmap
+    // fits the arena at once (the arena words were summed by k_classify)
+    size_t arena_cap = 0;
     if (tier_n[3] > 0) {
+        size_t free_b = 0, total_b = 0;
+        BEEP_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        arena_cap = std::max<size_t>((size_t)256 << 20, std::min<size_t>((size_t)48 << 30, free_b / 2));
+    }
+    if (tier_n[3] > 0 && large_words * 4 <= arena_cap) {
+        uint64_t *list = nullptr;
+        BEEP_TRY(make_list(3, list));
+        const uint32_t nl = tier_n[3];
+        unsigned long long *words, *boff;
+        uint32_t *chunks, *tasks, *cstart, *tstart, *arena;
+        BEEP_TRY(lp->alloc(words, nl));
+        BEEP_TRY(lp->alloc(boff, (size_t)nl + 1));
+        BEEP_TRY(lp->alloc(chunks, nl));
+        BEEP_TRY(lp->alloc(tasks, nl));
+        BEEP_TRY(lp->alloc(cstart, (size_t)nl + 1));
+        BEEP_TRY(lp->alloc(tstart, (size_t)nl + 1));
+        BEEP_TRY(lp->alloc(arena, std::max<uint64_t>(large_words, 32)));
+        const unsigned gl = std::max(1u, std::min(nl / 256 + 1, 1024u));
+        k_gather_dom<<<gl, 256, 0, s>>>(lp->d_pairs, list, nl, d_keys, d_sel);
+        k_large_meta<<<gl, 256, 0, s>>>(lp->d_pairs, list, nl, d_keys, d_sel, words, chunks, tasks);
+        st.kernel_launches += 2;
+        BEEP_CUDA_TRY(cudaGetLastError());
+        // exclusive prefixes with the total at [nl]
+        size_t tb = 0, tb2 = 0;
+        BEEP_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb, words, boff + 1, nl, s));
+        BEEP_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb2, chunks, cstart + 1, nl, s));
+        BEEP_TRY(ctx->grow(ctx->scratch, std::max(tb, tb2) + 1024));
+        tb = ctx->scratch.bytes;
+        BEEP_CUDA_TRY(cub::DeviceScan::InclusiveSum(ctx->scratch.ptr, tb, words, boff + 1, nl, s));
+        tb = ctx->scratch.bytes;
+        BEEP_CUDA_TRY(cub::DeviceScan::InclusiveSum(ctx->scratch.ptr, tb, chunks, cstart + 1, nl, s));
+        tb = ctx->scratch.bytes;
+        BEEP_CUDA_TRY(cub::DeviceScan::InclusiveSum(ctx->scratch.ptr, tb, tasks, tstart + 1, nl, s));
+        BEEP_CUDA_TRY(cudaMemsetAsync(boff, 0, 8, s));
+        BEEP_CUDA_TRY(cudaMemsetAsync(cstart, 0, 4, s));
+        BEEP_CUDA_TRY(cudaMemsetAsync(tstart, 0, 4, s));
+        const uint32_t maxD_all = tier_max[3];
+        const size_t smemA = std::min<size_t>(maxD_all, kLargeSmemA) * 4;
+        BEEP_CUDA_TRY(cudaFuncSetAttribute(k_large_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemA));
+        LaunchRec ms;
+        ms.kind = LaunchRec::kMemset;
+        ms.mptr = arena;
+        ms.mbytes = large_words * 4;
+        lp->recs.push_back(ms);
+        st.bitmap_bytes += large_words * 4;
+        LaunchRec lr;
+        lr.kind = LaunchRec::kLargeRows;
+        lr.grid = ctx->num_sms;
+        lr.block = 512;
+        lr.smem = smemA;
+        lr.bt = Batch{list, reinterpret_cast<const uint64_t *>(boff), cstart, tstart, nl};
+        lr.mptr = arena;
+        lr.cursor = cursor();
+        lr.sink = &st.large_encode_ms;
+        lp->recs.push_back(lr);
+        uint32_t first = 0;
+        for (int d = 3; d < kDepths; ++d) {
+            const uint32_t cnt = tier_depth[3 * kDepths + d];
+            if (!cnt)
+                continue;
+            LaunchRec ld;
+            ld.kind = LaunchRec::kLargeDfs;
+            ld.dend = d;
+            ld.grid = ctx->num_sms * 8;
+            ld.block = 256;
+            ld.bt = Batch{list + first, reinterpret_cast<const uint64_t *>(boff) + first, cstart, tstart + first,
+                          cnt};
+            ld.mptr = arena;
+            ld.cursor = cursor();
+            ld.sink = &st.large_dfs_ms;
+            lp->recs.push_back(ld);
+            first += cnt;
+        }
+    } else if (tier_n[3] > 0) {
+        // larger than the arena: batches planned on the host
         uint64_t *list = nullptr;
         BEEP_TRY(make_list(3, list));
         const uint32_t nl = tier_n[3];
@@ -1668,9 +1768,6 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             rs[i] = R{litems[i], D, lj[i], (uint32_t)pl.dend, words};
         }
         std::sort(rs.begin(), rs.end(), [](const R &a, const R &b) { return a.D > b.D; });
-        size_t free_b = 0, total_b = 0;
-        BEEP_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-        const size_t arena_cap = std::max<size_t>((size_t)256 << 20, std::min<size_t>((size_t)48 << 30, free_b / 2));
         // batch boundaries and the arena size (largest batch)
         std::vector<std::pair<size_t, size_t>> batches;
         size_t arena_words = 0;
