@@ -44,6 +44,8 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kSmallMaxD = 64;
 constexpr int kMediumAMaxD = 256;
 constexpr int kMediumMaxD = 1024;
+// 64-bit words per row of the thread-walker medium sub-tier (kMediumAMaxD bits)
+constexpr uint32_t kThreadNW = kMediumAMaxD / 64;
 
 struct ViewDev {
     const uint32_t *__restrict__ rp;
@@ -818,7 +820,6 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
         pair_domain(pr, r, beg, D, j0);
         const uint32_t rlo = pair_rlo(pr, D, j0);
         const uint32_t W = (D + 31) >> 5;
-        constexpr uint32_t kThreadNW = 4;                  // 64-bit words per row in thread mode
         const uint32_t row_words = G == 0 ? 2 * kThreadNW : W; // 32-bit words per row
         for (uint32_t i = threadIdx.x; i < D; i += blockDim.x)
             A[i] = pr.v.col[beg + i];
@@ -1876,7 +1877,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         BEEP_TRY(make_list(k, list));
         const uint32_t maxD = tier_max[k];
         // 32-bit words per row: 8 (4 x 64 bits) in the thread-mode sub-tier
-        const uint32_t W = sub == 0 ? 8u : (maxD + 31) / 32;
+        const uint32_t W = sub == 0 ? 2 * kThreadNW : (maxD + 31) / 32;
         const size_t pad = (maxD + 4) & ~3u;
         const size_t smem = (4 * pad + (size_t)maxD * W) * 4;
         const int block = sub == 0 ? 256 : 1024;
