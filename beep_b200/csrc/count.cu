@@ -349,12 +349,27 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
 // A group of G lanes (G = 32: a warp; gmask its lanes, glane the lane within
 // it) walks the words of a level G at a time; every lane of the group calls
 // this together.
-template <int P, int DEND, bool ENUM, int G = 32>
+//
+// LIST (large tier, G = 32): rows of cap > 0 carry, beside the bitmap, the
+// number of their non-zero words (nzc[i - rlo]) and, when that is at most
+// cap, the indices of those words in ascending order (nzl + (i - rlo) * cap).
+// A level then visits only the non-zero words of its sparsest back-edge row,
+// 32 a step: in a hub's neighbourhood a row has a few dozen bits among
+// hundreds of thousands, and the full scan costs ceil(D / 1024) warp steps
+// per level however few candidates there are.
+struct RowLists {
+    const uint32_t *nzc = nullptr; // non-zero words per row
+    const uint32_t *nzl = nullptr; // their indices, cap per row
+    uint32_t cap = 0;              // 0: no lists
+};
+
+template <int P, int DEND, bool ENUM, int G = 32, bool LIST = false>
 __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint32_t rlo, uint32_t W, uint32_t D,
                                          uint32_t (&x)[kMaxQ], unsigned long long &cnt, int glane, const EnumCtx &ec,
-                                         unsigned gmask = kFull) {
+                                         unsigned gmask = kFull, const RowLists &rl = RowLists()) {
     constexpr int LG = G == 32 ? 5 : (G == 16 ? 4 : (G == 8 ? 3 : (G == 4 ? 2 : (G == 2 ? 1 : 0))));
     static_assert((1 << LG) == G, "group size must be a power of two up to 32");
+    static_assert(!LIST || G == 32, "row lists are read by whole warps");
     const uint32_t bk = lp.back[P];
     const uint32_t lo = level_bound<P>(lp, x);
     bool closed = false; // group-uniform: count this level's candidates as C(A, DEND - P)
@@ -372,8 +387,40 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
     uint32_t acc = 0;
     const uint32_t nch = (W + G - 1) >> LG;
     const uint32_t tail = D & 31;
-    for (uint32_t ch = lo >> (5 + LG); ch < nch; ++ch) {
-        const uint32_t k = (ch << LG) + glane;
+    // Steps it0 .. it1 - 1 of G words each: consecutive words from the bound
+    // on, or (listed) the non-zero words of the sparsest back-edge row.
+    uint32_t it0 = lo >> (5 + LG), it1 = nch, nl = 0;
+    bool listed = false;
+    const uint32_t *bl = nullptr;
+    if constexpr (LIST) {
+        if (rl.cap) {
+            uint32_t best = 0xffffffffu;
+#pragma unroll
+            for (int q = 1; q < P; ++q)
+                if (bk >> q & 1u) {
+                    const uint32_t c = rl.nzc[x[q] - rlo];
+                    if (c < best) {
+                        best = c;
+                        bl = rl.nzl + (size_t)(x[q] - rlo) * rl.cap;
+                    }
+                }
+            if (best <= rl.cap) {
+                listed = true;
+                nl = best;
+                it0 = 0;
+                it1 = (best + G - 1) >> LG;
+            }
+        }
+    }
+    for (uint32_t it = it0; it < it1; ++it) {
+        // this lane's word (none when k >= W)
+        uint32_t k;
+        if (LIST && listed) {
+            const uint32_t e = (it << LG) + (uint32_t)glane;
+            k = e < nl ? bl[e] : 0xffffffffu;
+        } else {
+            k = (it << LG) + (uint32_t)glane;
+        }
         uint32_t w = 0;
         if (k < W) {
             w = (k + 1 < W || tail == 0) ? kFull : ((1u << tail) - 1u);
@@ -408,8 +455,11 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
                 const int b = __ffs(ww) - 1;
                 if (glane == L)
                     w &= w - 1;
-                x[P] = (((ch << LG) + (uint32_t)L) << 5) + (uint32_t)b;
-                dfs_warp<P + 1, DEND, ENUM, G>(lp, bm, rlo, W, D, x, cnt, glane, ec, gmask);
+                uint32_t kk = (it << LG) + (uint32_t)L;
+                if (LIST && listed)
+                    kk = __shfl_sync(gmask, k, L, G);
+                x[P] = (kk << 5) + (uint32_t)b;
+                dfs_warp<P + 1, DEND, ENUM, G, LIST>(lp, bm, rlo, W, D, x, cnt, glane, ec, gmask, rl);
                 bal = __ballot_sync(gmask, w != 0) >> gbase;
                 if constexpr (G < 32)
                     bal &= (1u << G) - 1u;
@@ -941,7 +991,28 @@ struct Batch {
 };
 
 constexpr uint32_t kRowsPerChunk = 256;
+constexpr int kLargeDfsBlocksPerSm = 8; // k_large_dfs grid: 256-thread blocks per SM
+// Depth slot of a root in the tier lists: its plan's depth, except the large
+// tier's 4-wheel roots, which take slot 2 (no plan has depth 2) and run on
+// k_large_wheel.
+constexpr uint32_t kWheelSlot = 2;
+__host__ __device__ __forceinline__ uint32_t depth_slot(const DevPlan &pl, uint32_t tier) {
+    return (tier == 4 && pl.wheel4) ? kWheelSlot : (uint32_t)pl.dend;
+}
 constexpr uint32_t kLargeSmemA = 48 * 1024; // domain entries staged in shared memory
+
+// Rows of at least kListMinW words also get non-zero-word lists of
+// W / 8 entries (rounded down to 32): 1 + W / 8 more words a row, under 13%.
+constexpr uint32_t kListMinW = 256;
+__host__ __device__ __forceinline__ uint32_t list_cap(uint32_t W) { return W >= kListMinW ? (W / 8) & ~31u : 0u; }
+
+// Arena words of one large root: rows [rlo, D) of W = ceil(D / 32) words,
+// then (list_cap(W) > 0) each row's non-zero word count and its list,
+// rounded up to 32 words.
+__host__ __device__ __forceinline__ uint64_t large_root_words(uint32_t D, uint32_t rlo) {
+    const uint32_t W = (D + 31) / 32, cap = list_cap(W);
+    return ((uint64_t)(D - rlo) * (W + (cap ? cap + 1 : 0)) + 31) & ~(uint64_t)31;
+}
 
 __device__ __forceinline__ uint32_t find_batch(const uint32_t *__restrict__ start, uint32_t nb, uint32_t t) {
     // last b with start[b] <= t
@@ -999,9 +1070,164 @@ __global__ void __launch_bounds__(512) k_large_rows(const PairDev *__restrict__ 
     }
 }
 
+// Non-zero-word counts and lists of the rows k_large_rows built (roots with
+// list_cap(W) > 0 only): a warp per row, 32 words a step. Blocks take the
+// 256-row chunks of the batch in turn.
+__global__ void __launch_bounds__(256) k_large_lists(const PairDev *__restrict__ pairs, Batch bt, uint32_t *arena) {
+    const uint32_t total = bt.cstart[bt.nb];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint32_t b = find_batch(bt.cstart, bt.nb, c);
+        const uint64_t it = bt.item[b];
+        PairRegs pr;
+        load_pair(pairs, item_pair(it), pr);
+        uint32_t beg, D, j0;
+        pair_domain(pr, item_root(it), beg, D, j0);
+        const uint32_t W = (D + 31) >> 5, cap = list_cap(W);
+        if (cap == 0)
+            continue;
+        const uint32_t rlo = pair_rlo(pr, D, j0);
+        const uint32_t *rows = arena + bt.off[b];
+        uint32_t *nzc = arena + bt.off[b] + (size_t)(D - rlo) * W;
+        uint32_t *nzl = nzc + (D - rlo);
+        const uint32_t i0 = max(rlo, (c - bt.cstart[b]) * kRowsPerChunk);
+        const uint32_t i1 = min(D, (c - bt.cstart[b] + 1) * kRowsPerChunk);
+        for (uint32_t i = i0 + warp; i < i1; i += nwarps) {
+            const uint32_t *row = rows + (size_t)(i - rlo) * W;
+            uint32_t *lst = nzl + (size_t)(i - rlo) * cap;
+            uint32_t n = 0;
+#pragma unroll 4
+            for (uint32_t k0 = 0; k0 < W; k0 += 32) {
+                const uint32_t k = k0 + (uint32_t)lane;
+                const uint32_t w = k < W ? row[k] : 0u;
+                const unsigned bal = __ballot_sync(kFull, w != 0);
+                const uint32_t pos = n + (uint32_t)__popc(bal & ((1u << lane) - 1u));
+                if (w != 0 && pos < cap)
+                    lst[pos] = k;
+                n += (uint32_t)__popc(bal);
+            }
+            if (lane == 0)
+                nzc[i - rlo] = n;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// the 4-wheel in closed form per (x1, x3) pair (large tier, counts only)
+// ---------------------------------------------------------------------------
+// Plan (the reference's chain for the 4-wheel): x2 in row(x1), x2 > x1;
+// x3 in row(x2), x3 > x1; x4 in row(x1) & row(x3), x4 > x1, x4 > x2. For a
+// fixed (x1, x3), x2 and x4 are two elements of S = row(x1) & row(x3) above
+// x1 with x2 < x4: C(|S|, 2) completions. A task (root, x1) therefore
+// collects the x3 > x1 that share a neighbour above x1 with x1 -- the OR U of
+// the rows of those neighbours, with the list of U's non-zero words -- and
+// counts S once per x3, instead of walking every (x2, x3) path: on R-MAT hub
+// neighbourhoods the paths outnumber the distinct pairs about 30 to 1.
+//
+// Scratch per warp (U zero on entry and left zero on exit): U and its word
+// list tl (W words each), and la (W words) for x1's non-zero words when its
+// row has no list. Rows are those of the whole domain (rlo = 0).
+__device__ __forceinline__ void wheel4_task(const uint32_t *__restrict__ bm, const RowLists &rl, uint32_t W,
+                                            uint32_t a, uint32_t *U, uint32_t *tl, uint32_t *la, int lane,
+                                            unsigned long long &cnt) {
+    const unsigned lt = (1u << lane) - 1u;
+    const uint32_t *ra = bm + (size_t)a * W;
+    const uint32_t aw = a >> 5;
+    const uint32_t above = ~((2u << (a & 31)) - 1u); // bits of word aw above a
+    // non-zero words of row(a) at or above aw: its list, or a scan into la
+    const uint32_t *al = la;
+    uint32_t na = 0;
+    if (rl.cap && rl.nzc[a] <= rl.cap) {
+        al = rl.nzl + (size_t)a * rl.cap;
+        na = rl.nzc[a];
+    } else {
+        for (uint32_t k0 = aw & ~31u; k0 < W; k0 += 32) {
+            const uint32_t k = k0 + (uint32_t)lane;
+            const uint32_t w = (k < W && k >= aw) ? ra[k] : 0u;
+            const unsigned bal = __ballot_sync(kFull, w != 0);
+            if (w)
+                la[na + (uint32_t)__popc(bal & lt)] = k;
+            na += (uint32_t)__popc(bal);
+        }
+        __syncwarp();
+    }
+    // U = OR over b in row(a), b > a, of row(b)'s bits above a; tl lists U's
+    // non-zero words
+    uint32_t nt = 0;
+    auto or_word = [&](const uint32_t *rb, uint32_t k) {
+        uint32_t v = 0;
+        if (k < W && k >= aw) {
+            v = rb[k];
+            if (k == aw)
+                v &= above;
+        }
+        bool fresh = false;
+        if (v) {
+            const uint32_t old = U[k];
+            fresh = old == 0;
+            U[k] = old | v;
+        }
+        const unsigned fb = __ballot_sync(kFull, fresh);
+        if (fresh)
+            tl[nt + (uint32_t)__popc(fb & lt)] = k;
+        nt += (uint32_t)__popc(fb);
+    };
+    for (uint32_t i = 0; i < na; ++i) {
+        const uint32_t e = al[i];
+        if (e < aw)
+            continue;
+        uint32_t wa = ra[e];
+        if (e == aw)
+            wa &= above;
+        while (wa) {
+            const uint32_t b = (e << 5) + (uint32_t)(__ffs(wa) - 1);
+            wa &= wa - 1;
+            const uint32_t *rb = bm + (size_t)b * W;
+            const uint32_t nb = rl.cap ? rl.nzc[b] : 0xffffffffu;
+            if (nb <= rl.cap) {
+                const uint32_t *bl = rl.nzl + (size_t)b * rl.cap;
+                for (uint32_t j0 = 0; j0 < nb; j0 += 32)
+                    or_word(rb, j0 + (uint32_t)lane < nb ? bl[j0 + lane] : 0xffffffffu);
+            } else {
+                for (uint32_t k0 = aw & ~31u; k0 < W; k0 += 32)
+                    or_word(rb, k0 + (uint32_t)lane);
+            }
+            __syncwarp(); // U's words visible to every lane before the next row
+        }
+    }
+    // every x3 of U: |S| over the shorter of the two word lists
+    for (uint32_t t0 = 0; t0 < nt; t0 += 32) {
+        uint32_t u = 0, k = 0;
+        if (t0 + (uint32_t)lane < nt) {
+            k = tl[t0 + lane];
+            u = U[k];
+            U[k] = 0;
+        }
+        while (u) {
+            const uint32_t c = (k << 5) + (uint32_t)(__ffs(u) - 1);
+            u &= u - 1;
+            const uint32_t *rc = bm + (size_t)c * W;
+            const uint32_t ncw = rl.cap ? rl.nzc[c] : 0xffffffffu;
+            const bool use_c = ncw <= rl.cap && ncw < na;
+            const uint32_t *lst = use_c ? rl.nzl + (size_t)c * rl.cap : al;
+            const uint32_t n = use_c ? ncw : na;
+            uint32_t s = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                const uint32_t e = lst[i];
+                if (e < aw)
+                    continue;
+                const uint32_t w = ra[e] & rc[e];
+                s += (uint32_t)__popc(e == aw ? (w & above) : w);
+            }
+            cnt += (unsigned long long)s * (s - (s ? 1u : 0u)) / 2;
+        }
+    }
+    __syncwarp(); // U back to zero before the warp's next task
+}
+
 template <int DEND, bool ENUM>
-__global__ void __launch_bounds__(256) k_large_dfs(const PairDev *__restrict__ pairs, Batch bt,
-                                                   const uint32_t *arena, unsigned *cursor) {
+__global__ void __launch_bounds__(256, (!ENUM && DEND <= 5) ? 3 : 1) k_large_dfs(const PairDev *__restrict__ pairs, Batch bt,
+                                                                      const uint32_t *arena, unsigned *cursor) {
     const int lane = threadIdx.x & 31;
     const uint32_t base0 = bt.tstart[0]; // the items' tasks are tstart[0] .. tstart[nb] - 1
     const uint32_t total = bt.tstart[bt.nb] - base0;
@@ -1039,7 +1265,60 @@ __global__ void __launch_bounds__(256) k_large_dfs(const PairDev *__restrict__ p
         }
         uint32_t x[kMaxQ];
         x[1] = j0 + (t - bt.tstart[b]);
-        dfs_warp<2, DEND, ENUM>(pr.lp, arena + bt.off[b], pair_rlo(pr, D, j0), W, D, x, cnt, lane, ec);
+        const uint32_t rlo = pair_rlo(pr, D, j0);
+        const uint32_t *rows = arena + bt.off[b];
+        RowLists rl;
+        rl.cap = list_cap(W);
+        rl.nzc = rows + (size_t)(D - rlo) * W;
+        rl.nzl = rl.nzc + (D - rlo);
+        dfs_warp<2, DEND, ENUM, 32, true>(pr.lp, rows, rlo, W, D, x, cnt, lane, ec, kFull, rl);
+    }
+    cnt = warp_sum(cnt);
+    if (lane == 0 && cnt)
+        atomicAdd(pr.count, cnt);
+}
+
+// The large tier's 4-wheel roots (classified into depth slot kWheelSlot):
+// every warp takes (root, x1) tasks from the cursor and runs wheel4_task on
+// its own scratch, wstride words at wsc + warp * wstride.
+__global__ void __launch_bounds__(256) k_large_wheel(const PairDev *__restrict__ pairs, Batch bt,
+                                                     const uint32_t *arena, unsigned *cursor, uint32_t *wsc,
+                                                     uint32_t wstride) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t base0 = bt.tstart[0];
+    const uint32_t total = bt.tstart[bt.nb] - base0;
+    uint32_t *ws = wsc + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * wstride;
+    PairRegs pr;
+    uint32_t cur = 0xffffffffu;
+    unsigned long long cnt = 0;
+    for (;;) {
+        uint32_t t = 0;
+        if (lane == 0)
+            t = atomicAdd(cursor, 1u);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= total)
+            break;
+        t += base0;
+        const uint32_t b = find_batch(bt.tstart, bt.nb, t);
+        const uint64_t it = bt.item[b];
+        const uint32_t p = item_pair(it), r = item_root(it);
+        if (p != cur) {
+            cnt = warp_sum(cnt);
+            if (lane == 0 && cnt)
+                atomicAdd(pr.count, cnt);
+            cnt = 0;
+            cur = p;
+            load_pair(pairs, p, pr);
+        }
+        uint32_t beg, D, j0;
+        pair_domain(pr, r, beg, D, j0);
+        const uint32_t W = (D + 31) >> 5;
+        const uint32_t *rows = arena + bt.off[b]; // rows of the whole domain: rlo == 0
+        RowLists rl;
+        rl.cap = list_cap(W);
+        rl.nzc = rows + (size_t)D * W;
+        rl.nzl = rl.nzc + D;
+        wheel4_task(rows, rl, W, j0 + (t - bt.tstart[b]), ws, ws + W, ws + 2 * (size_t)W, lane, cnt);
     }
     cnt = warp_sum(cnt);
     if (lane == 0 && cnt)
@@ -1255,11 +1534,11 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
         dom[t] = D;
         if (tc == 4) {
             const uint32_t rn = pd.pl.rows_needed, rlo = rn == 2 ? 0u : (rn == 1 ? j0 : D);
-            atomicAdd(large_words, ((uint64_t)(D - rlo) * ((D + 31) / 32) + 31) & ~(uint64_t)31);
+            atomicAdd(large_words, (unsigned long long)large_root_words(D, rlo));
         }
         if (tc) {
             mx[tc - 1] = max(mx[tc - 1], D);
-            atomicAdd(&s_hist[(tc - 1) * kDepths + pd.pl.dend], 1u);
+            atomicAdd(&s_hist[(tc - 1) * kDepths + depth_slot(pd.pl, tc)], 1u);
             if (tc == 1 && D <= cfg.tiny_max)
                 atomicAdd(&s_tiny[pd.pl.dend], 1u);
         }
@@ -1292,7 +1571,7 @@ __global__ void k_list_keys(const uint8_t *__restrict__ tier, const uint32_t *__
         uint32_t key = 0xffffffffu;
         if (tc) {
             const uint32_t p = find_pair(offs, npairs, t);
-            const uint32_t dend = (uint32_t)pairs[p].pl.dend;
+            const uint32_t dend = depth_slot(pairs[p].pl, tc);
             const uint32_t d = min(dom[t], kDomMask);
             const uint32_t dk = tc == 1 ? d : (tc == 5 ? 0u : kDomMask - d);
             key = ((tc - 1) << 28) | (dend << 24) | dk;
@@ -1321,7 +1600,7 @@ __global__ void k_large_meta(const PairDev *__restrict__ pairs, const uint64_t *
         const uint32_t D = D_in[i], j0 = j0_in[i];
         const uint32_t rn = (uint32_t)pairs[item_pair(items[i])].pl.rows_needed;
         const uint32_t rlo = rn == 2 ? 0u : (rn == 1 ? j0 : D);
-        words[i] = ((unsigned long long)(D - rlo) * ((D + 31) / 32) + 31) & ~31ull;
+        words[i] = large_root_words(D, rlo);
         chunks[i] = (D + kRowsPerChunk - 1) / kRowsPerChunk;
         tasks[i] = D - j0;
     }
@@ -1460,7 +1739,7 @@ beep_status launch_large_dfs(int dend, int grid, cudaStream_t s, const PairDev *
 // captured once into a CUDA graph (capture_plan) and relaunched.
 // ---------------------------------------------------------------------------
 struct LaunchRec {
-    enum Kind { kSmall, kMedium, kLargeRows, kLargeDfs, kGeneral, kMemset } kind;
+    enum Kind { kSmall, kMedium, kLargeRows, kLargeLists, kLargeDfs, kLargeWheel, kGeneral, kMemset } kind;
     const uint32_t *tstart = nullptr; // list walker: task prefix of the items
     int dend = 0, grid = 0, block = 0;
     int group = 32; // small tier: lanes per root
@@ -1471,8 +1750,21 @@ struct LaunchRec {
     Batch bt{};
     void *mptr = nullptr;
     size_t mbytes = 0;
-    double *sink = nullptr; // stats field this launch's time adds to
+    double *sink = nullptr;   // stats field this launch's time adds to
+    uint32_t *wsc = nullptr;  // large tier: 4-wheel scratch, wstride words a warp
+    uint32_t wstride = 0;
 };
+
+// The list pass over the rows a kLargeRows record builds.
+static LaunchRec lists_rec(const LaunchRec &rows) {
+    LaunchRec r = rows;
+    r.kind = LaunchRec::kLargeLists;
+    r.block = 256;
+    r.smem = 0;
+    r.grid = rows.grid * 4;
+    r.cursor = nullptr;
+    return r;
+}
 
 struct LaunchPlan {
     Ctx *ctx = nullptr;
@@ -1588,6 +1880,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     for (uint32_t i = 0; i < np; ++i) {
         hp[i].count = lp->d_counts + i;
         hp[i].en.n = lp->d_counts + np + i; // every pair has a valid tuple counter (k = 0: none written)
+        if (lp->enumerate)
+            hp[i].pl.wheel4 = 0; // the closed form counts; enumeration walks every match
     }
     BEEP_TRY(lp->alloc(lp->d_pairs, np));
     BEEP_TRY(lp->alloc(lp->d_offs, np + 1));
@@ -1672,6 +1966,22 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         BEEP_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
         arena_cap = std::max<size_t>((size_t)256 << 20, std::min<size_t>((size_t)48 << 30, free_b / 2));
     }
+    // scratch of the large tier's 4-wheel tasks: U, its word list and x1's
+    // words (W words each) for every warp of the DFS grid, zero on entry
+    uint32_t *wsc = nullptr;
+    uint32_t wstride = 0;
+    {
+        if (tier_depth[3 * kDepths + kWheelSlot] > 0) {
+            wstride = (3 * ((tier_max[3] + 31) / 32) + 31) & ~31u;
+            const size_t words = (size_t)ctx->num_sms * kLargeDfsBlocksPerSm * 8 * wstride;
+            BEEP_TRY(lp->alloc(wsc, words));
+            LaunchRec ms;
+            ms.kind = LaunchRec::kMemset;
+            ms.mptr = wsc;
+            ms.mbytes = words * 4;
+            lp->recs.push_back(ms);
+        }
+    }
     if (tier_n[3] > 0 && large_words * 4 <= arena_cap) {
         uint64_t *list = nullptr;
         BEEP_TRY(make_list(3, list));
@@ -1723,21 +2033,25 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         lr.cursor = cursor();
         lr.sink = &st.large_encode_ms;
         lp->recs.push_back(lr);
+        if (list_cap((maxD_all + 31) / 32))
+            lp->recs.push_back(lists_rec(lr));
         uint32_t first = 0;
-        for (int d = 3; d < kDepths; ++d) {
+        for (int d = (int)kWheelSlot; d < kDepths; ++d) {
             const uint32_t cnt = tier_depth[3 * kDepths + d];
             if (!cnt)
                 continue;
             LaunchRec ld;
-            ld.kind = LaunchRec::kLargeDfs;
+            ld.kind = d == (int)kWheelSlot ? LaunchRec::kLargeWheel : LaunchRec::kLargeDfs;
             ld.dend = d;
-            ld.grid = ctx->num_sms * 8;
+            ld.grid = ctx->num_sms * kLargeDfsBlocksPerSm;
             ld.block = 256;
             ld.bt = Batch{list + first, reinterpret_cast<const uint64_t *>(boff) + first, cstart, tstart + first,
                           cnt};
             ld.mptr = arena;
             ld.cursor = cursor();
             ld.sink = &st.large_dfs_ms;
+            ld.wsc = wsc;
+            ld.wstride = wstride;
             lp->recs.push_back(ld);
             first += cnt;
         }
@@ -1759,14 +2073,14 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         struct R {
             uint64_t item;
             uint32_t D, j0, dend;
-            uint64_t words; // bitmap rows [rlo, D) of D bits, rounded up to 32 words
+            uint64_t words; // bitmap rows [rlo, D) of D bits and their word lists
         };
         std::vector<R> rs(nl);
         for (uint32_t i = 0; i < nl; ++i) {
             const DevPlan &pl = hp[(uint32_t)(litems[i] >> 32)].pl;
             const uint32_t D = lD[i], rlo = pl.rows_needed == 2 ? 0u : (pl.rows_needed == 1 ? lj[i] : D);
-            const uint64_t words = ((uint64_t)(D - rlo) * ((D + 31) / 32) + 31) & ~(uint64_t)31;
-            rs[i] = R{litems[i], D, lj[i], (uint32_t)pl.dend, words};
+            const uint64_t words = large_root_words(D, rlo);
+            rs[i] = R{litems[i], D, lj[i], depth_slot(pl, 4), words};
         }
         std::sort(rs.begin(), rs.end(), [](const R &a, const R &b) { return a.D > b.D; });
         // batch boundaries and the arena size (largest batch)
@@ -1801,7 +2115,9 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             std::vector<uint64_t> bitem, boff;
             std::vector<uint32_t> cstart{0};
             uint64_t words = 0;
+            uint32_t bmaxD = 0;
             for (size_t i = i0; i < i1; ++i) {
+                bmaxD = std::max(bmaxD, rs[i].D);
                 bitem.push_back(rs[i].item);
                 boff.push_back(words);
                 words += rs[i].words;
@@ -1852,17 +2168,21 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             lr.cursor = cursor();
             lr.sink = &st.large_encode_ms;
             lp->recs.push_back(lr);
+            if (list_cap((bmaxD + 31) / 32))
+                lp->recs.push_back(lists_rec(lr));
             for (size_t gi = 0; gi < groups.size(); ++gi) {
                 LaunchRec ld;
-                ld.kind = LaunchRec::kLargeDfs;
                 ld.dend = (int)rs[i0 + groups[gi].first].dend;
-                ld.grid = ctx->num_sms * 8;
+                ld.kind = ld.dend == (int)kWheelSlot ? LaunchRec::kLargeWheel : LaunchRec::kLargeDfs;
+                ld.grid = ctx->num_sms * kLargeDfsBlocksPerSm;
                 ld.block = 256;
                 ld.bt = Batch{d_bitem + groups[gi].first, d_boff + groups[gi].first, d_cs, d_ts + ts_off[gi],
                               groups[gi].second};
                 ld.mptr = arena;
                 ld.cursor = cursor();
                 ld.sink = &st.large_dfs_ms;
+                ld.wsc = wsc;
+                ld.wstride = wstride;
                 lp->recs.push_back(ld);
             }
         }
@@ -2033,6 +2353,11 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats
             BEEP_CUDA_TRY(cudaGetLastError());
             st.large_encode_launches++;
             break;
+        case LaunchRec::kLargeLists:
+            k_large_lists<<<r.grid, r.block, 0, rs>>>(lp->d_pairs, r.bt, static_cast<uint32_t *>(r.mptr));
+            BEEP_CUDA_TRY(cudaGetLastError());
+            st.large_encode_launches++;
+            break;
         case LaunchRec::kLargeDfs:
             if (lp->enumerate)
                 BEEP_TRY(launch_large_dfs<true>(r.dend, r.grid, rs, lp->d_pairs, r.bt,
@@ -2040,6 +2365,12 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats
             else
                 BEEP_TRY(launch_large_dfs<false>(r.dend, r.grid, rs, lp->d_pairs, r.bt,
                                                  static_cast<const uint32_t *>(r.mptr), r.cursor));
+            st.large_dfs_launches++;
+            break;
+        case LaunchRec::kLargeWheel:
+            k_large_wheel<<<r.grid, r.block, 0, rs>>>(lp->d_pairs, r.bt, static_cast<const uint32_t *>(r.mptr),
+                                                      r.cursor, r.wsc, r.wstride);
+            BEEP_CUDA_TRY(cudaGetLastError());
             st.large_dfs_launches++;
             break;
         case LaunchRec::kMedium:

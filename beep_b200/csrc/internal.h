@@ -73,7 +73,7 @@ struct DevPlan {
     int32_t central;         // position 0 adjacent to every position (else: list walker)
     uint32_t adj0;           // bit p: position p is adjacent to position 0
     uint32_t sym0;           // bit p: position p must follow position 0
-    int32_t pad3;
+    int32_t wheel4;          // the 4-wheel's plan: counted per (x1, x3) pair in closed form
 };
 
 struct QueryPlan {

@@ -280,6 +280,13 @@ beep_status compile_plan(int32_t qn, const std::vector<int32_t> &rp, const std::
             if (P.sym[t] == 0)
                 D.sym0 |= 1u << p;
     }
+    // The 4-wheel: positions 1-4 a 4-cycle around the root (x2 ~ x1, x3 ~ x2,
+    // x4 ~ x1, x3) with the chain x2, x3, x4 > x1 and x4 > x2. Its count per
+    // (x1, x3) pair has a closed form, which the large tier uses.
+    D.wheel4 = (qn == 5 && D.dend == 5 && P.central && D.back[1] == 0 && D.back[2] == 0x2u &&
+                D.back[3] == 0x4u && D.back[4] == 0xAu && D.sym[2] == 0x2u && D.sym[3] == 0x2u && D.sym[4] == 0x6u)
+                   ? 1
+                   : 0;
     out->info = P;
     out->dev = D;
     return BEEP_OK;

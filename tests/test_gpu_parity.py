@@ -95,6 +95,42 @@ def test_large_tier_hub(ctx):
         g.close()
 
 
+def wide_hub_graph(seed):
+    """Hub 0 with 12,000 leaves (its neighbourhood rows are 12,000 bits wide,
+    so the large tier walks their non-zero-word lists), a sparse random graph
+    on the leaves, a second hub on 3,000 of them (a row too dense for its
+    list, walked word by word) and a 20-clique among the leaves."""
+    rng = np.random.default_rng(seed)
+    n = 12000
+    pairs = [(0, i) for i in range(1, n + 1)]
+    a = rng.integers(1, n + 1, size=48000)
+    b = rng.integers(1, n + 1, size=48000)
+    pairs += list(zip(a.tolist(), b.tolist()))
+    pairs += [(1, int(v)) for v in rng.choice(np.arange(2, n + 1), size=3000, replace=False)]
+    clique = rng.choice(np.arange(2, n + 1), size=20, replace=False).tolist()
+    pairs += list(itertools.combinations(clique, 2))
+    return csr_from_pairs(n + 1, pairs)
+
+
+def test_large_tier_word_lists(ctx):
+    rp, col = wide_hub_graph(5)
+    g = B.Graph.from_csr(ctx, rp, col)
+    try:
+        for name in ["w5", "diamond", "tailed_triangle", "k4", "k5", "triangle"]:
+            exp = O.count(rp, col, P.NAMED[name], apply_root_cap=False)["count"]
+            c, st = B.count(g, P.NAMED[name], B.SGM, B.OPT_TIMING, stats=True)
+            assert c == exp, name
+            if name in ("w5", "tailed_triangle"):
+                assert st["roots_large"] >= 1, (name, st)
+        # enumeration through the lists: the same set of matches as the oracle
+        total = O.count(rp, col, P.W5, apply_root_cap=False)["count"]
+        tuples, t = B.enumerate_matches(g, P.W5, total + 5)
+        assert t == total and len(tuples) == total
+        assert canon(tuples) == canon(O.enumerate_matches(rp, col, P.W5))
+    finally:
+        g.close()
+
+
 @pytest.mark.parametrize("scale,ef,seed", [(12, 8, 1), (14, 6, 2)])
 def test_rmat_named_patterns(ctx, scale, ef, seed):
     rp, col = B.gen_rmat(scale, ef, 0.57, 0.19, 0.19, seed)
