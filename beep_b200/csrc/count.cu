@@ -725,6 +725,92 @@ template <int G> __device__ __forceinline__ unsigned long long group_sum(unsigne
     return v;
 }
 
+// ---------------------------------------------------------------------------
+// the 4-wheel in closed form on shared-memory rows (small and medium tiers)
+// ---------------------------------------------------------------------------
+// The same count as wheel4_task (large tier) for one x1 = a: U = OR of the
+// rows of a's neighbours above a, then C(|row(a) & row(x3) above a|, 2) for
+// every x3 of U above a. Rows of the whole domain (rlo = 0).
+// One thread, rows of NW 64-bit words: row(a) and U stay in registers.
+template <int NW>
+__device__ __forceinline__ unsigned long long wheel4_thread(const uint64_t *rows, uint32_t a) {
+    uint64_t ra[NW], U[NW];
+    const uint32_t aw = a >> 6;
+    const uint64_t above = ~((2ull << (a & 63)) - 1ull); // bits of word aw above a
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        const uint64_t w = rows[(size_t)a * NW + k];
+        ra[k] = (uint32_t)k > aw ? w : ((uint32_t)k == aw ? (w & above) : 0ull);
+        U[k] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        uint64_t w = ra[k];
+        while (w) {
+            const uint32_t b = (uint32_t)k * 64 + (uint32_t)(__ffsll((long long)w) - 1);
+            w &= w - 1;
+#pragma unroll
+            for (int kk = 0; kk < NW; ++kk)
+                U[kk] |= rows[(size_t)b * NW + kk];
+        }
+    }
+    unsigned long long cnt = 0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        uint64_t u = (uint32_t)k > aw ? U[k] : ((uint32_t)k == aw ? (U[k] & above) : 0ull);
+        while (u) {
+            const uint32_t c = (uint32_t)k * 64 + (uint32_t)(__ffsll((long long)u) - 1);
+            u &= u - 1;
+            uint32_t n = 0;
+#pragma unroll
+            for (int kk = 0; kk < NW; ++kk)
+                n += (uint32_t)__popcll(ra[kk] & rows[(size_t)c * NW + kk]);
+            cnt += (unsigned long long)n * (n - (n ? 1u : 0u)) / 2;
+        }
+    }
+    return cnt;
+}
+
+// One warp, rows of W <= 32 32-bit words (lane k holds word k); the count is
+// returned on lane 0.
+__device__ __forceinline__ unsigned long long wheel4_warp(const uint32_t *rows, uint32_t W, uint32_t a, int lane) {
+    const uint32_t k = (uint32_t)lane;
+    const uint32_t aw = a >> 5;
+    const uint32_t above = ~((2u << (a & 31)) - 1u);
+    auto hi = [&](uint32_t w) { return k > aw ? w : (k == aw ? (w & above) : 0u); };
+    const uint32_t ra = k < W ? hi(rows[(size_t)a * W + k]) : 0u;
+    uint32_t U = 0, w = ra;
+    unsigned bal = __ballot_sync(kFull, w != 0);
+    while (bal) {
+        const int L = __ffs(bal) - 1;
+        const uint32_t ww = __shfl_sync(kFull, w, L);
+        const uint32_t b = ((uint32_t)L << 5) + (uint32_t)(__ffs(ww) - 1);
+        if (lane == L)
+            w &= w - 1;
+        if (k < W)
+            U |= rows[(size_t)b * W + k];
+        bal = __ballot_sync(kFull, w != 0);
+    }
+    uint32_t u = k < W ? hi(U) : 0u;
+    unsigned long long cnt = 0;
+    bal = __ballot_sync(kFull, u != 0);
+    while (bal) {
+        const int L = __ffs(bal) - 1;
+        const uint32_t uu = __shfl_sync(kFull, u, L);
+        const uint32_t c = ((uint32_t)L << 5) + (uint32_t)(__ffs(uu) - 1);
+        if (lane == L)
+            u &= u - 1;
+        uint32_t n = k < W ? (uint32_t)__popc(ra & rows[(size_t)c * W + k]) : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            n += __shfl_xor_sync(kFull, n, o);
+        if (lane == 0)
+            cnt += (unsigned long long)n * (n - (n ? 1u : 0u)) / 2;
+        bal = __ballot_sync(kFull, u != 0);
+    }
+    return cnt;
+}
+
 template <int DEND, bool ENUM, int G, int MAXD>
 __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(const PairDev *__restrict__ pairs,
                                                            const uint64_t *__restrict__ items, uint32_t nitems) {
@@ -743,6 +829,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
     uint32_t cur = 0xffffffffu;
     EnumCtx ec;
     unsigned long long cnt = 0;
+    bool wheel = false; // the 4-wheel's closed form (counts)
     for (uint32_t ri = blockIdx.x * NG + gid; ri < nitems; ri += gridDim.x * NG) {
         const uint64_t it = items[ri];
         const uint32_t p = item_pair(it), r = item_root(it);
@@ -755,6 +842,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
             load_pair(pairs, p, pr);
             if constexpr (ENUM)
                 make_ec(ec, pairs[p].en, pairs[p].pl, pr.v);
+            wheel = DEND == 5 && !ENUM && pairs[p].pl.wheel4;
         }
         uint32_t beg, D, j0;
         pair_domain(pr, r, beg, D, j0);
@@ -777,7 +865,10 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
             ec.A = A;
             ec.root = r;
         }
-        if (DEND == 3 || pr.lp.free_from <= 2) { // group-uniform
+        if (wheel) { // group-uniform; rows of the whole domain
+            for (uint32_t j = j0 + glane; j < D; j += G)
+                cnt += wheel4_thread<1>(rows, j);
+        } else if (DEND == 3 || pr.lp.free_from <= 2) { // group-uniform
             for (uint32_t j = j0 + glane; j < D; j += G) {
                 uint32_t x[kMaxQ];
                 x[1] = j;
@@ -847,6 +938,7 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
     uint32_t cur = 0xffffffffu;
     EnumCtx ec;
     unsigned long long cnt = 0;
+    bool wheel = false; // the 4-wheel's closed form (counts)
     for (;;) {
         if (threadIdx.x == 0)
             s_ri = atomicAdd(cursor, 1u);
@@ -865,6 +957,7 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
             load_pair(pairs, p, pr);
             if constexpr (ENUM)
                 make_ec(ec, pairs[p].en, pairs[p].pl, pr.v);
+            wheel = DEND == 5 && !ENUM && pairs[p].pl.wheel4;
         }
         uint32_t beg, D, j0;
         pair_domain(pr, r, beg, D, j0);
@@ -905,7 +998,14 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
         }
         if constexpr (G == 0) {
             const uint64_t *r64 = reinterpret_cast<const uint64_t *>(rows);
-            if (DEND == 3 || pr.lp.free_from <= 2) { // block-uniform
+            if (wheel) { // block-uniform; rows of the whole domain
+                for (;;) {
+                    const uint32_t j = atomicAdd(&s_j, 1u);
+                    if (j >= D)
+                        break;
+                    cnt += wheel4_thread<kThreadNW>(r64, j);
+                }
+            } else if (DEND == 3 || pr.lp.free_from <= 2) { // block-uniform
                 // level 2 is the last or is counted in closed form: O(1) per level-1 vertex
                 for (;;) {
                     const uint32_t j = atomicAdd(&s_j, 1u);
@@ -967,6 +1067,12 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
                 j = __shfl_sync(gmask, j, 0, G);
                 if (j >= D)
                     break;
+                if constexpr (G == 32) {
+                    if (wheel) { // block-uniform; rows of the whole domain
+                        cnt += wheel4_warp(rows, W, j, glane);
+                        continue;
+                    }
+                }
                 uint32_t x[kMaxQ];
                 x[1] = j;
                 dfs_warp<2, DEND, ENUM, G>(pr.lp, rows, rlo, W, D, x, cnt, glane, ec, gmask);
