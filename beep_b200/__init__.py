@@ -72,6 +72,7 @@ class PlanInfo(ctypes.Structure):
         ("aut_order", ctypes.c_int32),
         ("restricted", ctypes.c_int32),
         ("central", ctypes.c_int32),
+        ("wheel4", ctypes.c_int32),
     ]
 
 
@@ -384,6 +385,7 @@ class Query:
             "aut_order": p.aut_order,
             "restricted": p.restricted,
             "central": p.central,
+            "wheel4": p.wheel4,
         }
 
     def close(self) -> None:

@@ -280,13 +280,32 @@ beep_status compile_plan(int32_t qn, const std::vector<int32_t> &rp, const std::
             if (P.sym[t] == 0)
                 D.sym0 |= 1u << p;
     }
-    // The 4-wheel: positions 1-4 a 4-cycle around the root (x2 ~ x1, x3 ~ x2,
-    // x4 ~ x1, x3) with the chain x2, x3, x4 > x1 and x4 > x2. Its count per
-    // (x1, x3) pair has a closed form, which the large tier uses.
-    D.wheel4 = (qn == 5 && D.dend == 5 && P.central && D.back[1] == 0 && D.back[2] == 0x2u &&
-                D.back[3] == 0x4u && D.back[4] == 0xAu && D.sym[2] == 0x2u && D.sym[3] == 0x2u && D.sym[4] == 0x6u)
-                   ? 1
-                   : 0;
+    // The 4-wheel: positions 1-4 a 4-cycle around the root. When its chain
+    // puts every other position after x1 and x1's two cycle neighbours in
+    // order (no other constraint, none against the root at position 1), x1 is
+    // the cycle's first vertex and the completions of (x1, opposite vertex c)
+    // are C(|row(x1) & row(c) above x1|, 2); the kernels sum that per pair.
+    // The reference's chain takes this form under the labellings of the
+    // 4-wheel seen so far (x2 ~ x1 ~ x4, or x2 ~ x1 ~ x3).
+    D.wheel4 = 0;
+    if (qn == 5 && D.dend == 5 && P.central && D.pos1_after_root == 0) {
+        uint32_t adj[5] = {0, 0, 0, 0, 0};
+        for (int p = 2; p <= 4; ++p)
+            for (int q = 1; q < p; ++q)
+                if (D.back[p] >> q & 1u) {
+                    adj[p] |= 1u << q;
+                    adj[q] |= 1u << p;
+                }
+        bool cycle = true; // four vertices of degree 2: a 4-cycle
+        for (int p = 1; p <= 4; ++p)
+            cycle = cycle && __builtin_popcount(adj[p]) == 2;
+        if (cycle) {
+            const int n1 = __builtin_ctz(adj[1]), n2 = 31 - __builtin_clz(adj[1]);
+            const int o = 2 + 3 + 4 - n1 - n2;
+            D.wheel4 = (D.sym[n1] == 0x2u && D.sym[o] == 0x2u && D.sym[n2] == (0x2u | 1u << n1)) ? 1 : 0;
+        }
+    }
+    P.wheel4 = D.wheel4;
     out->info = P;
     out->dev = D;
     return BEEP_OK;

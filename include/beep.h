@@ -142,6 +142,8 @@ typedef struct beep_plan_info {
                               reference's requirement, README.md:51-53); 0: counted by the
                               list-intersection walker (sgm, or sgc without an unmatched
                               last position) */
+    int32_t wheel4;        /* 1: the 4-wheel's plan (positions 1-4 a 4-cycle around the
+                              root); counts are summed once per (x1, x3) pair in closed form */
 } beep_plan_info;
 beep_status beep_query_plan(const beep_query *q, beep_mode mode, beep_plan_info *out);
 

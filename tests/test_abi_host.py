@@ -2,6 +2,7 @@
 include/beep.h declares, the query compiler agrees with the oracle, file
 formats and generators behave. No device calls. CPU only."""
 import ctypes
+import itertools
 import os
 import re
 import struct
@@ -63,6 +64,23 @@ def test_restricted_flag():
     assert B.Query.from_edges(P.TRIANGLE).plan()["restricted"] == 1
     assert B.Query.from_edges(P.DIAMOND).plan()["restricted"] == 0
     assert B.Query.from_edges(P.W5).plan()["restricted"] == 0
+
+
+def test_wheel4_flag():
+    """Only the 4-wheel's plan takes the per-(x1, x3) closed form: under every
+    labelling of its edge list (the reference's chain comes out in two forms)
+    and in both modes (its last position is adjacent to the one before, so
+    sgc counts full matches)."""
+    plans = set()
+    for perm in itertools.permutations(range(5)):
+        pl = B.Query.from_edges([(perm[a], perm[b]) for a, b in P.W5]).plan()
+        assert pl["wheel4"] == 1
+        plans.add((tuple(pl["qedge"]), tuple(pl["sym"])))
+    assert len(plans) == 2
+    assert B.Query.from_edges(P.W5).plan(B.SGC)["wheel4"] == 1
+    for q in [P.K4, P.DIAMOND, P.TAILED_TRIANGLE, P.TRIANGLE] + P.central_patterns(5):
+        pl = B.Query.from_edges(q).plan()
+        assert pl["wheel4"] == (1 if pl["qdeg"] == [4, 3, 3, 3, 3] and pl["aut_order"] == 8 else 0), q
 
 
 def test_unsupported_queries_fail_cleanly(built):

@@ -116,11 +116,16 @@ def test_large_tier_word_lists(ctx):
     rp, col = wide_hub_graph(5)
     g = B.Graph.from_csr(ctx, rp, col)
     try:
-        for name in ["w5", "diamond", "tailed_triangle", "k4", "k5", "triangle"]:
-            exp = O.count(rp, col, P.NAMED[name], apply_root_cap=False)["count"]
-            c, st = B.count(g, P.NAMED[name], B.SGM, B.OPT_TIMING, stats=True)
+        # the 4-wheel under its second labelling too (the other form of the reference's chain)
+        w5b = P.central_patterns(5)[8]
+        assert B.Query.from_edges(w5b).plan()["wheel4"] == 1 and sorted(w5b) != sorted(P.W5)
+        queries = {name: P.NAMED[name] for name in ["w5", "diamond", "tailed_triangle", "k4", "k5", "triangle"]}
+        queries["w5_relabelled"] = w5b
+        for name, q in queries.items():
+            exp = O.count(rp, col, q, apply_root_cap=False)["count"]
+            c, st = B.count(g, q, B.SGM, B.OPT_TIMING, stats=True)
             assert c == exp, name
-            if name in ("w5", "tailed_triangle"):
+            if name in ("w5", "w5_relabelled", "tailed_triangle"):
                 assert st["roots_large"] >= 1, (name, st)
         # enumeration through the lists: the same set of matches as the oracle
         total = O.count(rp, col, P.W5, apply_root_cap=False)["count"]
