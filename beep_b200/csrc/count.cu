@@ -18,15 +18,19 @@
 //     vertices, minus bits below the symmetry bound) while the enumeration
 //     state lives in registers, unrolled over the compile-time depth;
 //   - the next candidate comes from __ballot_sync + __ffs across the warp;
-//   - the last level is a popcount (as in the reference).
-// Three tiers by domain size D:
-//   small   D <= 64   warp per root, 64-bit rows in shared memory, one lane per
-//                     level-1 vertex (thread-level DFS);
-//   medium  D <= 1024 block per root, rows in shared memory, warps take
-//                     level-1 vertices from a shared counter;
+//   - the last level is a popcount (as in the reference); free suffixes and
+//     the 4-wheel are counted in closed form.
+// Tiers by domain size D (limits are runtime parameters, defaults shown):
+//   small   D <= 64   a group of 8 or 32 lanes per root, 64-bit rows in shared
+//                     memory, a lane per level-1 vertex or (level-1, level-2)
+//                     pair (thread-level DFS);
+//   medium  D <= 1024 block per root, rows in shared memory, a thread (D <= 256)
+//                     or a warp per level-1 vertex;
 //   large   D > 1024  rows in a global arena; one launch builds the rows of a
-//                     batch of roots, a second spreads the (root, level-1 vertex)
+//                     batch of roots (and a second the non-zero-word lists of
+//                     wide rows), a third spreads the (root, level-1 vertex)
 //                     tasks over every warp of the GPU.
+// Queries without a central vertex take a fifth, list-walking tier.
 #include <algorithm>
 #include <cmath>
 #include <mutex>
