@@ -52,3 +52,7 @@ def test_closed_form_equals_the_walk(built, gen, args):
     rp, col = {"er": B.gen_erdos_renyi, "cl": B.gen_chung_lu, "rmat": B.gen_rmat}[gen](*args)
     exp = O.count(rp, col, P.W5, apply_root_cap=False)["count"]
     assert wheel_pairs_count(rp, col) == exp
+    # the oracle walks the other form of the chain (another labelling) to the same count
+    w5b = P.central_patterns(5)[8]
+    assert sorted(w5b) != sorted(P.W5)
+    assert O.count(rp, col, w5b, apply_root_cap=False)["count"] == exp
