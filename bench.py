@@ -326,7 +326,8 @@ def bench_batched(args):
     from beep_b200 import patterns as P
 
     specs = c4_graph_specs(args.c4_graphs, 10, args.c4_max_scale, 8, args.c4_max_degree)
-    ctx = B.Context(0)
+    stream = torch.cuda.Stream()
+    ctx = B.Context(0, cuda_stream=stream.cuda_stream)
     t0 = time.perf_counter()
     host = [B.gen_chung_lu(*sp) for sp in specs]
     gen_s = time.perf_counter() - t0
@@ -353,17 +354,29 @@ def bench_batched(args):
     t0 = time.perf_counter()
     first = batch.run()  # plans and captures
     plan_s = time.perf_counter() - t0
+    clocks = ClockSampler(0)
+    clocks.start()
     for _ in range(args.warmup):
         batch.run()
-    times = []
+    times, host_times = [], []
     for _ in range(args.steps):
+        # device time of one replay on the library's stream (CUDA events), and
+        # the host time of the call around it
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
+        e0.record(stream)
         got = batch.run()
-        times.append(time.perf_counter() - t0)
+        e1.record(stream)
+        e1.synchronize()
+        host_times.append(time.perf_counter() - t0)
+        times.append(e0.elapsed_time(e1) / 1e3)
+    clk = clocks.stop()
     assert got == first and sum(got) == plain_total, "batched counts differ from the plain loop"
     step_s = statistics.median(times)
     line = {"metric": METRIC, "impl": "ours", "form": "batched", "value": sum(got) / step_s, "unit": UNIT,
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+            "host_ms_per_step": statistics.median(host_times) * 1e3, "clocks": clk,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": WORKLOADS["c4"]["desc"], "graphs": len(graphs), "patterns": len(pats),
                        "pairs": len(pairs), "n_log2_range": [10, args.c4_max_scale],
