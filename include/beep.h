@@ -177,10 +177,12 @@ typedef struct beep_stats {
     int32_t kernel_launches;    /* kernels this call launched */
     double prep_ms;             /* device time: peel + ordering (BEEP_OPT_TIMING) */
     double count_ms;            /* device time: counting kernels */
+    /* per tier (BEEP_OPT_TIMING); large_encode: row builds and word lists,
+     * large_dfs: the large tier's walks and 4-wheel kernels */
     double small_ms, medium_ms, large_encode_ms, large_dfs_ms;
     int32_t small_launches, medium_launches, large_encode_launches, large_dfs_launches;
     uint64_t adjacency_bytes;   /* adjacency bytes the kernels must read (BEEP_OPT_ALG_BYTES) */
-    uint64_t bitmap_bytes;      /* neighbourhood bitmap bytes of the large tier */
+    uint64_t bitmap_bytes;      /* bitmap arena bytes of the large tier (rows and word lists) */
     uint64_t small_bytes, medium_bytes, large_bytes; /* adjacency_bytes by tier (BEEP_OPT_ALG_BYTES) */
     int64_t roots_general;      /* roots of non-central queries (list walker) */
     double general_ms;
