@@ -27,7 +27,12 @@ HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "beep.h")
 MAX_QUERY = 10
 
 # beep_status
-OK, ERR_INVALID_ARG, ERR_IO, ERR_PARSE, ERR_UNSUPPORTED, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_TIMEOUT, ERR_INTERNAL = range(9)
+(OK, ERR_INVALID_ARG, ERR_IO, ERR_PARSE, ERR_UNSUPPORTED, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_TIMEOUT, ERR_INTERNAL,
+ ERR_OVERFLOW) = range(10)
+# counts are exact below COUNT_LIMIT; a batch slot holds COUNT_OVERFLOW for a count at or above it
+COUNT_LIMIT = 0xFFF0000000000000
+COUNT_OVERFLOW = 0xFFFFFFFFFFFFFFFF
+NOALLOC_MAX_DOMAIN = 23168
 # beep_mode
 SGM, SGC = 0, 1
 # options
@@ -47,7 +52,7 @@ class BeepError(RuntimeError):
 
 def _status_name(s: int) -> str:
     names = ["ok", "invalid argument", "i/o error", "parse error", "unsupported", "cuda error", "out of memory",
-             "timeout", "internal error"]
+             "timeout", "internal error", "count overflow"]
     return names[s] if 0 <= s < len(names) else f"status {s}"
 
 
@@ -122,7 +127,7 @@ class Stats(ctypes.Structure):
         ("roots_general", ctypes.c_int64),
         ("general_ms", ctypes.c_double),
         ("general_launches", ctypes.c_int32),
-        ("pad0", ctypes.c_int32),
+        ("overflow_pairs", ctypes.c_int32),
         ("alg_small_bytes", ctypes.c_uint64),
         ("alg_medium_bytes", ctypes.c_uint64),
         ("alg_large_bytes", ctypes.c_uint64),
@@ -542,13 +547,14 @@ def count_noalloc(device: int, n: int, m: int, d_row_ptr: int, d_col_ind: int, q
 
 
 def count_shard(graph: Graph, query, shard: int, nshards: int, mode: int = SGM, options: int = 0,
-                ctx: Context | None = None) -> int:
-    """Count of the roots whose input vertex id % nshards == shard."""
+                ctx: Context | None = None, stats: bool = False):
+    """Count of the roots whose input vertex id % nshards == shard. With
+    stats=True returns (count, stats dict)."""
     q = _as_query(query)
     st = Stats()
     _check(lib().beep_count_shard(ctx.handle if ctx else None, graph.handle, q.handle, int(mode), int(options),
                                   int(shard), int(nshards), ctypes.byref(st)))
-    return int(st.count)
+    return (int(st.count), st.as_dict()) if stats else int(st.count)
 
 
 def enumerate_matches(graph: Graph, query, k: int, ctx: Context | None = None):

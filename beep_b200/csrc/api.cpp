@@ -22,6 +22,14 @@ beep_status fail(beep_status s, const std::string &msg) {
 
 namespace {
 
+// BEEP_ERR_OVERFLOW when a single-pair call's count reached BEEP_COUNT_LIMIT.
+beep_status overflow_status(const beep_stats &st) {
+    if (st.count != BEEP_COUNT_OVERFLOW)
+        return BEEP_OK;
+    return fail(BEEP_ERR_OVERFLOW, "the count is at least BEEP_COUNT_LIMIT (2^64 - 2^52) and is not representable "
+                                   "as an exact u64");
+}
+
 beep_status bind(beep_ctx *ctx) {
     if (!ctx)
         return fail(BEEP_ERR_INVALID_ARG, "null context");
@@ -106,6 +114,8 @@ const char *beep_status_string(beep_status s) {
         return "timeout";
     case BEEP_ERR_INTERNAL:
         return "internal error";
+    case BEEP_ERR_OVERFLOW:
+        return "count overflow";
     }
     return "unknown";
 }
@@ -386,7 +396,7 @@ beep_status beep_count_ex(beep_ctx *ctx, beep_graph *g, const beep_query *q, bee
     ctx->impl.launches += (uint64_t)st.kernel_launches;
     if (stats)
         *stats = st;
-    return BEEP_OK;
+    return overflow_status(st);
 }
 
 beep_status beep_count_shard(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t options,
@@ -407,16 +417,17 @@ beep_status beep_count_shard(beep_ctx *ctx, beep_graph *g, const beep_query *q, 
     ctx->impl.launches += (uint64_t)st.kernel_launches;
     if (stats)
         *stats = st;
-    return BEEP_OK;
+    return overflow_status(st);
 }
 
 beep_status beep_count(beep_ctx *ctx, beep_graph *g, const beep_query *q, beep_mode mode, uint64_t *out_count) {
     if (!out_count)
         return fail(BEEP_ERR_INVALID_ARG, "beep_count: null output");
     beep_stats st;
-    BEEP_TRY(beep_count_ex(ctx, g, q, mode, 0, &st));
-    *out_count = st.count;
-    return BEEP_OK;
+    const beep_status rc = beep_count_ex(ctx, g, q, mode, 0, &st);
+    if (rc == BEEP_OK || rc == BEEP_ERR_OVERFLOW)
+        *out_count = st.count;
+    return rc;
 }
 
 beep_status beep_enumerate(beep_ctx *ctx, beep_graph *g, const beep_query *q, uint64_t k, int32_t *out_tuples,
@@ -437,6 +448,12 @@ beep_status beep_enumerate(beep_ctx *ctx, beep_graph *g, const beep_query *q, ui
     beep_stats st;
     BEEP_TRY(run_count(&ctx->impl, &g->impl, p, 0, k > 0 ? &er : nullptr, &st));
     ctx->impl.launches += (uint64_t)st.kernel_launches;
+    if (st.count == BEEP_COUNT_OVERFLOW) {
+        *n_out = 0;
+        if (total_count)
+            *total_count = st.count;
+        return overflow_status(st);
+    }
     const uint64_t got = std::min<uint64_t>(k, st.count);
     if (got)
         BEEP_CUDA_TRY(cudaMemcpyAsync(out_tuples, dout.ptr, got * K * 4, cudaMemcpyDeviceToHost, ctx->impl.stream));

@@ -84,16 +84,51 @@ __device__ __forceinline__ Lp load_lp(const DevPlan &pl) {
     return lp;
 }
 
-// C(A, L) for L <= 4, exact through a 128-bit product (A < 2^32), reduced
-// mod 2^64 like every count here.
-__device__ __forceinline__ unsigned long long binom_le4(uint32_t A, int L) {
+// ---------------------------------------------------------------------------
+// count overflow. A pair's count is a u64 (the reference's counter,
+// subgraph_matching.cuh:1277, wraps silently). Here counts of kCountLimit =
+// 2^64 - 2^52 or more are reported as overflow instead:
+//   - closed-form terms (C(A, L), wheel pair terms) are added saturating: a
+//     lane counter that would reach the limit is set to it;
+//   - leaf popcounts (at most 64 each) are added unchecked: between two
+//     flushes a lane adds fewer than 2^51 that way (2^45 additions take a
+//     lane more than nine hours), so a saturated counter stays below 2^64;
+//   - flushes sum lanes saturating and check the global add for a carry.
+// A pair's counter is two words: the count, then a flag set on overflow.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kCountLimit = BEEP_COUNT_LIMIT;
+static_assert(BEEP_COUNT_LIMIT == 0ull - (1ull << 52), "count limit");
+
+__device__ __forceinline__ unsigned long long sat_add(unsigned long long a, unsigned long long b) {
+    const unsigned long long s = a + b;
+    return (s < a || s >= kCountLimit) ? kCountLimit : s;
+}
+
+// cnt + C(A, L) for L <= 4, the binomial exact through a 128-bit product
+// (A < 2^32), saturating at kCountLimit.
+__device__ __forceinline__ unsigned long long add_binom(unsigned long long cnt, uint32_t A, int L) {
     if (A < (uint32_t)L)
-        return 0ull;
+        return cnt;
     unsigned __int128 num = 1;
     for (int i = 0; i < L; ++i)
         num *= (unsigned __int128)(A - (uint32_t)i);
     const uint32_t fact = L <= 1 ? 1u : (L == 2 ? 2u : (L == 3 ? 6u : 24u));
-    return (unsigned long long)(num / fact);
+    const unsigned __int128 s = num / fact + (unsigned __int128)cnt;
+    return s >= (unsigned __int128)kCountLimit ? kCountLimit : (unsigned long long)s;
+}
+
+// Adds a flushed (saturated) sum to a pair's counter; sets its overflow flag
+// (the word after the count) when the sum or the new total reaches the limit.
+__device__ __forceinline__ void flush_count(unsigned long long *pc, unsigned long long v) {
+    if (v >= kCountLimit) {
+        atomicOr(pc + 1, 1ull);
+        return;
+    }
+    if (!v)
+        return;
+    const unsigned long long old = atomicAdd(pc, v);
+    if (old + v < old || old + v >= kCountLimit)
+        atomicOr(pc + 1, 1ull);
 }
 
 // Positions P..DEND-1 form a free suffix when they share one back-edge set B
@@ -285,7 +320,7 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
         if constexpr (!ENUM && DEND - P <= 4) {
             if (suffix_applies<P, DEND>(lp, x, lo)) {
                 if (lp.free_back == 0) {
-                    cnt += binom_le4(free_count_rootonly<P>(D, x, lo), DEND - P);
+                    cnt = add_binom(cnt, free_count_rootonly<P>(D, x, lo), DEND - P);
                     return;
                 }
                 closed = DEND - P >= 2; // one level: the leaf popcount below is the same
@@ -295,7 +330,7 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
             // one word: the candidate set stays in a register
             uint64_t c = cand_word<P, 1>(lp, rows, rlo, D, lo, x, 0);
             if (closed) {
-                cnt += binom_le4((uint32_t)__popcll(c), DEND - P);
+                cnt = add_binom(cnt, (uint32_t)__popcll(c), DEND - P);
                 return;
             }
             if constexpr (P == DEND - 1) {
@@ -321,7 +356,7 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
                     emit_bits(ec, x, P, w, k * 64);
                 A += (uint32_t)__popcll(w);
             }
-            cnt += closed ? binom_le4(A, DEND - P) : (unsigned long long)A;
+            cnt = closed ? add_binom(cnt, A, DEND - P) : cnt + (unsigned long long)A;
             return;
         }
         if constexpr (P < DEND - 1 && NW > 1) {
@@ -381,7 +416,7 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
         if (suffix_applies<P, DEND>(lp, x, lo)) {
             if (lp.free_back == 0) {
                 if (glane == 0)
-                    cnt += binom_le4(free_count_rootonly<P>(D, x, lo), DEND - P);
+                    cnt = add_binom(cnt, free_count_rootonly<P>(D, x, lo), DEND - P);
                 return;
             }
             closed = DEND - P >= 2; // one level: the leaf popcount below is the same
@@ -476,14 +511,15 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
         for (int o = G / 2; o > 0; o >>= 1)
             A += __shfl_xor_sync(gmask, A, o, G);
         if (glane == 0)
-            cnt += binom_le4(A, DEND - P);
+            cnt = add_binom(cnt, A, DEND - P);
     }
 }
 
+// Sum over the warp, saturating at kCountLimit (every lane gets it).
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(kFull, v, o);
+        v = sat_add(v, __shfl_xor_sync(kFull, v, o));
     return v;
 }
 
@@ -725,7 +761,7 @@ constexpr int kTinyMaxD = 16;
 template <int G> __device__ __forceinline__ unsigned long long group_sum(unsigned long long v, unsigned gmask) {
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1)
-        v += __shfl_xor_sync(gmask, v, o, G);
+        v = sat_add(v, __shfl_xor_sync(gmask, v, o, G));
     return v;
 }
 
@@ -769,7 +805,7 @@ __device__ __forceinline__ unsigned long long wheel4_thread(const uint64_t *rows
 #pragma unroll
             for (int kk = 0; kk < NW; ++kk)
                 n += (uint32_t)__popcll(ra[kk] & rows[(size_t)c * NW + kk]);
-            cnt += (unsigned long long)n * (n - (n ? 1u : 0u)) / 2;
+            cnt = sat_add(cnt, (unsigned long long)n * (n - (n ? 1u : 0u)) / 2);
         }
     }
     return cnt;
@@ -809,7 +845,7 @@ __device__ __forceinline__ unsigned long long wheel4_warp(const uint32_t *rows, 
         for (int o = 16; o > 0; o >>= 1)
             n += __shfl_xor_sync(kFull, n, o);
         if (lane == 0)
-            cnt += (unsigned long long)n * (n - (n ? 1u : 0u)) / 2;
+            cnt = sat_add(cnt, (unsigned long long)n * (n - (n ? 1u : 0u)) / 2);
         bal = __ballot_sync(kFull, u != 0);
     }
     return cnt;
@@ -839,8 +875,8 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
         const uint32_t p = item_pair(it), r = item_root(it);
         if (p != cur) { // group-uniform
             cnt = group_sum<G>(cnt, gmask);
-            if (glane == 0 && cnt)
-                atomicAdd(pr.count, cnt);
+            if (glane == 0)
+                flush_count(pr.count, cnt);
             cnt = 0;
             cur = p;
             load_pair(pairs, p, pr);
@@ -871,7 +907,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
         }
         if (wheel) { // group-uniform; rows of the whole domain
             for (uint32_t j = j0 + glane; j < D; j += G)
-                cnt += wheel4_thread<1>(rows, j);
+                cnt = sat_add(cnt, wheel4_thread<1>(rows, j));
         } else if (DEND == 3 || pr.lp.free_from <= 2) { // group-uniform
             for (uint32_t j = j0 + glane; j < D; j += G) {
                 uint32_t x[kMaxQ];
@@ -911,8 +947,8 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
         __syncwarp(gmask);
     }
     cnt = group_sum<G>(cnt, gmask);
-    if (glane == 0 && cnt)
-        atomicAdd(pr.count, cnt);
+    if (glane == 0)
+        flush_count(pr.count, cnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -954,8 +990,8 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
         const uint32_t p = item_pair(it), r = item_root(it);
         if (p != cur) { // block-uniform
             cnt = warp_sum(cnt);
-            if (lane == 0 && cnt)
-                atomicAdd(pr.count, cnt);
+            if (lane == 0)
+                flush_count(pr.count, cnt);
             cnt = 0;
             cur = p;
             load_pair(pairs, p, pr);
@@ -1007,7 +1043,7 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
                     const uint32_t j = atomicAdd(&s_j, 1u);
                     if (j >= D)
                         break;
-                    cnt += wheel4_thread<kThreadNW>(r64, j);
+                    cnt = sat_add(cnt, wheel4_thread<kThreadNW>(r64, j));
                 }
             } else if (DEND == 3 || pr.lp.free_from <= 2) { // block-uniform
                 // level 2 is the last or is counted in closed form: O(1) per level-1 vertex
@@ -1073,7 +1109,7 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
                     break;
                 if constexpr (G == 32) {
                     if (wheel) { // block-uniform; rows of the whole domain
-                        cnt += wheel4_warp(rows, W, j, glane);
+                        cnt = sat_add(cnt, wheel4_warp(rows, W, j, glane));
                         continue;
                     }
                 }
@@ -1085,8 +1121,8 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
         __syncthreads();
     }
     cnt = warp_sum(cnt);
-    if (lane == 0 && cnt)
-        atomicAdd(pr.count, cnt);
+    if (lane == 0)
+        flush_count(pr.count, cnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -1329,7 +1365,7 @@ __device__ __forceinline__ void wheel4_task(const uint32_t *__restrict__ bm, con
                 const uint32_t w = ra[e] & rc[e];
                 s += (uint32_t)__popc(e == aw ? (w & above) : w);
             }
-            cnt += (unsigned long long)s * (s - (s ? 1u : 0u)) / 2;
+            cnt = sat_add(cnt, (unsigned long long)s * (s - (s ? 1u : 0u)) / 2);
         }
     }
     __syncwarp(); // U back to zero before the warp's next task
@@ -1358,8 +1394,8 @@ __global__ void __launch_bounds__(256, (!ENUM && DEND <= 5) ? 3 : 1) k_large_dfs
         const uint32_t p = item_pair(it), r = item_root(it);
         if (p != cur) {
             cnt = warp_sum(cnt);
-            if (lane == 0 && cnt)
-                atomicAdd(pr.count, cnt);
+            if (lane == 0)
+                flush_count(pr.count, cnt);
             cnt = 0;
             cur = p;
             load_pair(pairs, p, pr);
@@ -1384,8 +1420,8 @@ __global__ void __launch_bounds__(256, (!ENUM && DEND <= 5) ? 3 : 1) k_large_dfs
         dfs_warp<2, DEND, ENUM, 32, true>(pr.lp, rows, rlo, W, D, x, cnt, lane, ec, kFull, rl);
     }
     cnt = warp_sum(cnt);
-    if (lane == 0 && cnt)
-        atomicAdd(pr.count, cnt);
+    if (lane == 0)
+        flush_count(pr.count, cnt);
 }
 
 // The large tier's 4-wheel roots (classified into depth slot kWheelSlot):
@@ -1414,8 +1450,8 @@ __global__ void __launch_bounds__(256) k_large_wheel(const PairDev *__restrict__
         const uint32_t p = item_pair(it), r = item_root(it);
         if (p != cur) {
             cnt = warp_sum(cnt);
-            if (lane == 0 && cnt)
-                atomicAdd(pr.count, cnt);
+            if (lane == 0)
+                flush_count(pr.count, cnt);
             cnt = 0;
             cur = p;
             load_pair(pairs, p, pr);
@@ -1431,8 +1467,8 @@ __global__ void __launch_bounds__(256) k_large_wheel(const PairDev *__restrict__
         wheel4_task(rows, rl, W, j0 + (t - bt.tstart[b]), ws, ws + W, ws + 2 * (size_t)W, lane, cnt);
     }
     cnt = warp_sum(cnt);
-    if (lane == 0 && cnt)
-        atomicAdd(pr.count, cnt);
+    if (lane == 0)
+        flush_count(pr.count, cnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -1556,8 +1592,7 @@ __global__ void __launch_bounds__(256) k_general(const PairDev *__restrict__ pai
         const uint64_t it = items[b];
         const uint32_t p = item_pair(it), r = item_root(it);
         if (p != cur) {
-            if (cnt)
-                atomicAdd(count_ptr, cnt);
+            flush_count(count_ptr, cnt);
             cnt = 0;
             cur = p;
             load_gen(pairs[p], g);
@@ -1569,8 +1604,8 @@ __global__ void __launch_bounds__(256) k_general(const PairDev *__restrict__ pai
         x[1] = g.v.col[g.v.rp[r] + j0 + (t + base0 - tstart[b])];
         gen_walk<2, DEND, ENUM>(g, x, cnt);
     }
-    if (cnt)
-        atomicAdd(count_ptr, cnt);
+    if (count_ptr)
+        flush_count(count_ptr, cnt);
 }
 
 // task counts (D - j0) of listed items
@@ -1886,10 +1921,13 @@ struct LaunchPlan {
     uint64_t *d_offs = nullptr;
     uint8_t *d_tier = nullptr;
     uint64_t N = 0;
-    unsigned long long *d_counts = nullptr; // np counts, np tuple counters, 4 byte counters
+    // per pair (count, overflow flag), then np tuple counters, then kAux byte counters
+    unsigned long long *d_counts = nullptr;
     unsigned *d_cursors = nullptr;
     uint32_t ncursors = 0;
-    unsigned long long *h_counts = nullptr; // pinned mirror (np + kAux): the context's buffer, or owned when captured
+    // pinned mirror of the (count, flag) words and the byte counters (2 np + kAux):
+    // the context's buffer, or owned when captured
+    unsigned long long *h_counts = nullptr;
     bool own_h_counts = false;
     std::vector<LaunchRec> recs;
     bool enumerate = false;
@@ -1918,6 +1956,12 @@ struct LaunchPlan {
 };
 
 void LaunchPlanDeleter::operator()(LaunchPlan *p) const { delete p; }
+
+// Pair i's count after the read-back: BEEP_COUNT_OVERFLOW when its overflow
+// flag is set.
+static uint64_t pair_result(const LaunchPlan *lp, uint32_t i) {
+    return lp->h_counts[2 * (size_t)i + 1] ? BEEP_COUNT_OVERFLOW : lp->h_counts[2 * (size_t)i];
+}
 
 beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out,
                        const TierCfg &tiers) {
@@ -1975,8 +2019,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     const uint32_t np = (uint32_t)hp.size();
     lp->np = np;
     tr.mark("views");
-    BEEP_TRY(ctx->host_results(np + kAux, &lp->h_counts));
-    BEEP_TRY(lp->alloc(lp->d_counts, 2 * (size_t)np + kAux));
+    BEEP_TRY(ctx->host_results(2 * (size_t)np + kAux, &lp->h_counts));
+    BEEP_TRY(lp->alloc(lp->d_counts, 3 * (size_t)np + kAux));
     lp->ncursors = 64;
     BEEP_TRY(lp->alloc(lp->d_cursors, lp->ncursors));
     if (np == 0) {
@@ -1988,8 +2032,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         return fail(BEEP_ERR_UNSUPPORTED, "more than 2^32 vertices in one call");
     lp->N = N;
     for (uint32_t i = 0; i < np; ++i) {
-        hp[i].count = lp->d_counts + i;
-        hp[i].en.n = lp->d_counts + np + i; // every pair has a valid tuple counter (k = 0: none written)
+        hp[i].count = lp->d_counts + 2 * (size_t)i;
+        hp[i].en.n = lp->d_counts + 2 * (size_t)np + i; // every pair has a valid tuple counter (k = 0: none written)
         if (lp->enumerate)
             hp[i].pl.wheel4 = 0; // the closed form counts; enumeration walks every match
     }
@@ -2425,7 +2469,7 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats
                   std::vector<double *> *sinks) {
     cudaStream_t s = ctx->stream;
     const uint32_t np = lp->np;
-    BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_counts, 0, (2 * (size_t)np + kAux) * 8, s));
+    BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_counts, 0, (3 * (size_t)np + kAux) * 8, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_cursors, 0, lp->ncursors * 4, s));
     // The tiers are independent: large on the call's stream, medium and small
     // on two side streams forked from it and joined back at the end.
@@ -2540,7 +2584,7 @@ beep_status capture_plan(Ctx *ctx, LaunchPlan *lp) {
     // the captured read-back needs a host buffer that no other call reuses
     if (!lp->own_h_counts) {
         unsigned long long *h = nullptr;
-        BEEP_CUDA_TRY(cudaMallocHost(&h, (lp->np + kAux) * sizeof(unsigned long long)));
+        BEEP_CUDA_TRY(cudaMallocHost(&h, (2 * (size_t)lp->np + kAux) * sizeof(unsigned long long)));
         lp->h_counts = h;
         lp->own_h_counts = true;
     }
@@ -2549,7 +2593,7 @@ beep_status capture_plan(Ctx *ctx, LaunchPlan *lp) {
     cudaGraph_t graph = nullptr;
     BEEP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     beep_status rc = issue(ctx, lp, false, false, scratch_st, nullptr, nullptr);
-    cudaError_t ce = cudaMemcpyAsync(lp->h_counts, lp->d_counts, (lp->np + 4) * 8, cudaMemcpyDeviceToHost, s);
+    cudaError_t ce = cudaMemcpyAsync(lp->h_counts, lp->d_counts, 2 * (size_t)lp->np * 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamEndCapture(s, &graph);
     if (rc != BEEP_OK) {
         if (graph)
@@ -2586,18 +2630,18 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
     } else {
         st.kernel_launches = lp->st.kernel_launches;
         BEEP_TRY(issue(ctx, lp, timing, (options & BEEP_OPT_SERIAL_TIERS) != 0, st, &ev, &sinks));
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, (lp->np + 4) * 8, cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, 2 * (size_t)lp->np * 8, cudaMemcpyDeviceToHost, s));
     }
     if (timing)
         cudaEventRecord(e1, s);
     if (lp->np > 0 && (options & BEEP_OPT_ALG_BYTES)) {
-        unsigned long long *d_bytes = lp->d_counts + 2 * (size_t)lp->np;
+        unsigned long long *d_bytes = lp->d_counts + 3 * (size_t)lp->np;
         BEEP_CUDA_TRY(cudaMemsetAsync(d_bytes, 0, kAux * 8, s));
         const int gv = std::max(1, (int)std::min<uint64_t>((lp->N + 255) / 256, (uint64_t)ctx->num_sms * 32));
         k_alg_bytes<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, lp->np, lp->d_tier, lp->N, d_bytes);
         BEEP_CUDA_TRY(cudaGetLastError());
         st.kernel_launches += 1;
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts + lp->np, d_bytes, kAux * 8, cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts + 2 * (size_t)lp->np, d_bytes, kAux * 8, cudaMemcpyDeviceToHost, s));
     }
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     if (timing) {
@@ -2624,19 +2668,27 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
     for (size_t i = 0; i < ncounts; ++i)
         counts[i] = 0;
     st.count = 0;
+    st.overflow_pairs = 0;
     for (uint32_t i = 0; i < lp->np; ++i) {
+        const uint64_t c = pair_result(lp, i);
         if (lp->live[i] < ncounts)
-            counts[lp->live[i]] = lp->h_counts[i];
-        st.count += lp->h_counts[i];
+            counts[lp->live[i]] = c;
+        if (c == BEEP_COUNT_OVERFLOW)
+            ++st.overflow_pairs;
+        st.count = (st.count == BEEP_COUNT_OVERFLOW || c == BEEP_COUNT_OVERFLOW || st.count + c < st.count ||
+                    st.count + c >= BEEP_COUNT_LIMIT)
+                       ? BEEP_COUNT_OVERFLOW
+                       : st.count + c;
     }
     if (options & BEEP_OPT_ALG_BYTES) {
-        st.small_bytes = lp->h_counts[lp->np + 0];
-        st.medium_bytes = lp->h_counts[lp->np + 1];
-        st.large_bytes = lp->h_counts[lp->np + 2];
+        const unsigned long long *aux = lp->h_counts + 2 * (size_t)lp->np;
+        st.small_bytes = aux[0];
+        st.medium_bytes = aux[1];
+        st.large_bytes = aux[2];
         st.adjacency_bytes = st.small_bytes + st.medium_bytes + st.large_bytes;
-        st.alg_small_bytes = lp->h_counts[lp->np + 3];
-        st.alg_medium_bytes = lp->h_counts[lp->np + 4];
-        st.alg_large_bytes = lp->h_counts[lp->np + 5];
+        st.alg_small_bytes = aux[3];
+        st.alg_medium_bytes = aux[4];
+        st.alg_large_bytes = aux[5];
     }
     if (stats)
         *stats = st;
@@ -2646,21 +2698,22 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
 beep_status launch_plan_async(Ctx *ctx, LaunchPlan *lp) {
     if (!lp->own_h_counts) {
         unsigned long long *h = nullptr;
-        BEEP_CUDA_TRY(cudaMallocHost(&h, (lp->np + kAux) * sizeof(unsigned long long)));
+        BEEP_CUDA_TRY(cudaMallocHost(&h, (2 * (size_t)lp->np + kAux) * sizeof(unsigned long long)));
         lp->h_counts = h;
         lp->own_h_counts = true;
     }
     beep_stats st;
     std::memset(&st, 0, sizeof(st));
     BEEP_TRY(issue(ctx, lp, false, false, st, nullptr, nullptr));
-    BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, (lp->np + 4) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, 2 * (size_t)lp->np * 8, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
     return BEEP_OK;
 }
 
 uint64_t plan_count(const LaunchPlan *lp, size_t spec_index) {
     for (uint32_t i = 0; i < lp->np; ++i)
         if (lp->live[i] == spec_index)
-            return lp->h_counts[i];
+            return pair_result(lp, i);
     return 0;
 }
 
@@ -2742,10 +2795,21 @@ constexpr size_t kNoAllocCtrlBytes = 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[BEEP_NOALLOC_SCRATCH_BYTES];
 
 struct NoAllocCtrl {
-    unsigned long long count;
+    unsigned long long count;    // the match count ...
+    unsigned long long overflow; // ... and its overflow flag (the word after it)
     unsigned int cursor;
     unsigned int max_domain;
+    unsigned int bad_csr;        // bit 0: row pointers, bit 1: column entries
 };
+static_assert(sizeof(NoAllocCtrl) <= kNoAllocCtrlBytes, "control block");
+
+// Largest search domain whose bitmap (D rows of ceil(D / 32) words, the slice
+// rounded up to 64 words) fits the scratch array after the control block.
+constexpr uint64_t noalloc_slice_words(uint64_t D) { return (D * ((D + 31) / 32) + 63) & ~(uint64_t)63; }
+constexpr uint64_t kNoAllocArenaWords = (BEEP_NOALLOC_SCRATCH_BYTES - kNoAllocCtrlBytes) / 4;
+static_assert(noalloc_slice_words(BEEP_NOALLOC_MAX_DOMAIN) <= kNoAllocArenaWords &&
+                  noalloc_slice_words(BEEP_NOALLOC_MAX_DOMAIN + 1) > kNoAllocArenaWords,
+              "BEEP_NOALLOC_MAX_DOMAIN is the largest domain whose bitmap fits the scratch array");
 
 // Root domain straight from a sorted, simple CSR in vertex-id order.
 __device__ __forceinline__ void csr_root_domain(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
@@ -2770,18 +2834,40 @@ __device__ __forceinline__ bool csr_is_root(const DevPlan &pl, uint32_t deg, uin
     return deg >= min_deg && D + 1 >= (uint32_t)pl.dend && j0 < D;
 }
 
+// A warp per row: checks the caller's CSR (row pointers non-decreasing
+// within [0, m]; entries below n, strictly increasing, no self loop) before
+// any kernel uses an entry as an index, and takes the largest search domain
+// of the valid rows. Entries of a row are read only when its pointers are
+// valid, so a bad CSR is reported, never read out of bounds.
 __global__ void k_noalloc_maxdom(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, int64_t n,
-                                 DevPlan pl, uint32_t min_deg, NoAllocCtrl *ctrl) {
-    uint32_t mx = 0;
-    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t beg, D, j0, deg;
-        csr_root_domain(rp, col, pl, (uint32_t)v, beg, D, j0, deg);
-        if (csr_is_root(pl, deg, D, j0, min_deg))
-            mx = max(mx, D);
+                                 int64_t m, DevPlan pl, uint32_t min_deg, NoAllocCtrl *ctrl) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    uint32_t mx = 0, bad = 0;
+    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+        const uint32_t b = rp[v], e = rp[v + 1];
+        if (b > e || (int64_t)e > m || (v == 0 && b != 0)) {
+            bad |= 1u;
+            continue;
+        }
+        for (uint32_t i = b + lane; i < e; i += 32) {
+            const uint32_t w = col[i];
+            if (!((int64_t)w < n && w != (uint32_t)v && (i == b || col[i - 1] < w)))
+                bad |= 2u;
+        }
+        if (lane == 0) {
+            uint32_t beg, D, j0, deg;
+            csr_root_domain(rp, col, pl, (uint32_t)v, beg, D, j0, deg);
+            if (csr_is_root(pl, deg, D, j0, min_deg))
+                mx = max(mx, D);
+        }
     }
     mx = __reduce_max_sync(kFull, mx);
-    if ((threadIdx.x & 31) == 0 && mx)
+    bad = __reduce_or_sync(kFull, bad);
+    if (lane == 0 && mx)
         atomicMax(&ctrl->max_domain, mx);
+    if (lane == 0 && bad)
+        atomicOr(&ctrl->bad_csr, bad);
 }
 
 // Rows [i0, i1) of the domain A (size D) of a root, ids ascending: the
@@ -2887,8 +2973,8 @@ __global__ void __launch_bounds__(512) k_noalloc_count(const uint32_t *__restric
         __syncthreads();
     }
     cnt = warp_sum(cnt);
-    if (lane == 0 && cnt)
-        atomicAdd(&ctrl->count, cnt);
+    if (lane == 0)
+        flush_count(&ctrl->count, cnt);
 }
 
 std::mutex g_noalloc_mu;
@@ -2945,29 +3031,37 @@ extern "C" beep_status beep_count_noalloc(int device, void *cuda_stream, int64_t
     BEEP_CUDA_TRY(cudaMemsetAsync(scratch, 0, kNoAllocCtrlBytes, s));
     const uint32_t min_deg = (uint32_t)plan.info.max_qdeg;
     if (n > 0) {
-        const int g0 = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms * 16));
-        k_noalloc_maxdom<<<g0, 256, 0, s>>>(rp, col, n, pl, min_deg, ctrl);
+        const int g0 = (int)std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, (int64_t)num_sms * 16));
+        k_noalloc_maxdom<<<g0, 256, 0, s>>>(rp, col, n, m, pl, min_deg, ctrl);
         BEEP_CUDA_TRY(cudaGetLastError());
     }
-    uint32_t maxD = 0;
-    BEEP_CUDA_TRY(cudaMemcpyAsync(&maxD, &ctrl->max_domain, sizeof(maxD), cudaMemcpyDeviceToHost, s));
+    uint32_t h_ctrl[2] = {0, 0}; // max_domain, bad_csr
+    BEEP_CUDA_TRY(cudaMemcpyAsync(h_ctrl, &ctrl->max_domain, sizeof(h_ctrl), cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    const uint32_t maxD = h_ctrl[0];
+    if (h_ctrl[1] & 1u)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_count_noalloc: row_ptr must start at 0 and be non-decreasing "
+                                          "within [0, m]");
+    if (h_ctrl[1] & 2u)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_count_noalloc: every row must hold strictly increasing vertex ids "
+                                          "below n with no self loop");
     if (maxD == 0) {
         *out_count = 0;
         return BEEP_OK;
     }
     const uint32_t smem_maxD = (uint32_t)kMediumMaxD;
-    const uint64_t arena_words = (BEEP_NOALLOC_SCRATCH_BYTES - kNoAllocCtrlBytes) / 4;
+    const uint64_t arena_words = kNoAllocArenaWords;
     uint64_t slice_words = 0;
     int grid = num_sms;
     if (maxD > smem_maxD) {
-        slice_words = ((uint64_t)maxD * ((maxD + 31) / 32) + 63) & ~(uint64_t)63;
-        if (slice_words > arena_words)
+        slice_words = noalloc_slice_words(maxD);
+        if (maxD > BEEP_NOALLOC_MAX_DOMAIN)
             return fail(BEEP_ERR_UNSUPPORTED,
                         "beep_count_noalloc: the largest search domain has " + std::to_string(maxD) +
                             " vertices; its bitmap needs " + std::to_string(slice_words * 4) +
                             " bytes, more than the " + std::to_string(BEEP_NOALLOC_SCRATCH_BYTES) +
-                            "-byte scratch of the allocation-free path (domains up to 23170 vertices); use beep_count");
+                            "-byte scratch of the allocation-free path (domains up to " +
+                            std::to_string(BEEP_NOALLOC_MAX_DOMAIN) + " vertices); use beep_count");
         grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms, arena_words / slice_words));
     }
     const size_t pad = (smem_maxD + 4) & ~3u;
@@ -2993,9 +3087,13 @@ extern "C" beep_status beep_count_noalloc(int device, void *cuda_stream, int64_t
         return fail(BEEP_ERR_UNSUPPORTED, "depth out of range");
     }
     BEEP_CUDA_TRY(cudaGetLastError());
-    unsigned long long c = 0;
-    BEEP_CUDA_TRY(cudaMemcpyAsync(&c, &ctrl->count, sizeof(c), cudaMemcpyDeviceToHost, s));
+    unsigned long long c[2] = {0, 0}; // count, overflow flag
+    BEEP_CUDA_TRY(cudaMemcpyAsync(c, &ctrl->count, sizeof(c), cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
-    *out_count = c;
+    if (c[1]) {
+        *out_count = BEEP_COUNT_OVERFLOW;
+        return fail(BEEP_ERR_OVERFLOW, "beep_count_noalloc: the count is at least BEEP_COUNT_LIMIT (2^64 - 2^52)");
+    }
+    *out_count = c[0];
     return BEEP_OK;
 }

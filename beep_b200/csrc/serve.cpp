@@ -102,11 +102,15 @@ void Server::finish(Slot &sl, beep_status st, const std::string &err) {
             r.error = err;
         } else {
             r.count = plan_count(sl.plan.get(), i);
-            if (r.k > 0) {
+            if (r.count == BEEP_COUNT_OVERFLOW) {
+                r.status = BEEP_ERR_OVERFLOW;
+                r.error = "the count is at least BEEP_COUNT_LIMIT (2^64 - 2^52)";
+            } else if (r.k > 0) {
                 r.n_tuples = std::min<uint64_t>(r.k, r.count);
                 r.tuples.assign(sl.hbufs[i], sl.hbufs[i] + r.n_tuples * (uint64_t)r.plan.info.K);
             }
-            matches += r.count;
+            if (r.status == BEEP_OK)
+                matches += r.count;
         }
         lat_ms.push_back(ms_between(r.arrival, r.done));
         r.finished = true;

@@ -41,8 +41,16 @@ typedef enum beep_status {
     BEEP_ERR_CUDA = 5,          /* CUDA runtime error (message has the CUDA error string) */
     BEEP_ERR_OUT_OF_MEMORY = 6, /* device or host allocation failed / admission refused */
     BEEP_ERR_TIMEOUT = 7,       /* a bounded device wait ran out */
-    BEEP_ERR_INTERNAL = 8
+    BEEP_ERR_INTERNAL = 8,
+    BEEP_ERR_OVERFLOW = 9       /* the count is BEEP_COUNT_LIMIT or more: not representable */
 } beep_status;
+
+/* Counts are exact below BEEP_COUNT_LIMIT = 2^64 - 2^52. A count at or above
+ * it is reported as overflow (BEEP_ERR_OVERFLOW from the single-pair calls,
+ * BEEP_COUNT_OVERFLOW in a batch's count slot) rather than reduced mod 2^64
+ * as the reference's u64 counter is (subgraph_matching.cuh:1277). */
+#define BEEP_COUNT_LIMIT 0xFFF0000000000000ull
+#define BEEP_COUNT_OVERFLOW 0xFFFFFFFFFFFFFFFFull
 
 /* MAINTASK values GRAPH_MATCH ("sgm") and GRAPH_COUNT ("sgc")
  * (include/defs.cuh:78-95, include/Config.h:80-84). */
@@ -187,7 +195,8 @@ typedef struct beep_stats {
     int64_t roots_general;      /* roots of non-central queries (list walker) */
     double general_ms;
     int32_t general_launches;
-    int32_t pad0;
+    int32_t overflow_pairs;     /* pairs whose count reached BEEP_COUNT_LIMIT (count is then
+                                   BEEP_COUNT_OVERFLOW, also in the aggregate) */
     /* BEEP_OPT_ALG_BYTES: algorithmic bytes of the searched roots by tier,
      * 4 * (deg r + sum of deg v over v in N(r)) on the input CSR -- the
      * adjacency traffic of building each root's neighbourhood bitmap from the
@@ -310,6 +319,9 @@ beep_status beep_serve_destroy(beep_server *s);
 /* Size of the device scratch array the allocation-free path uses (64 MiB per
  * device, held from the first call until the process exits). */
 #define BEEP_NOALLOC_SCRATCH_BYTES (64u << 20)
+/* Largest search domain (vertices) whose bitmap fits that array: D rows of
+ * ceil(D / 32) words must fit (64 MiB - 256 B) / 4 words. */
+#define BEEP_NOALLOC_MAX_DOMAIN 23168u
 
 /* Count matches without allocating any device memory. No counterpart in the
  * reference: it exists for callers that cannot let a library call cudaMalloc
@@ -321,8 +333,12 @@ beep_status beep_serve_destroy(beep_server *s);
  * Input: the caller's CSR in device memory on `device` (rows sorted
  * ascending, no duplicate edge, no self loop, both directions -- the form
  * beep_graph_csr returns); output: the count written to *out_count (host).
- * Work is ordered on cuda_stream (NULL: the legacy default stream) and the
- * call returns when it is done. It calls no cudaMalloc, cudaFree or other
+ * The CSR is checked on the device before it is used: row pointers that are
+ * not non-decreasing within [0, m], entries at or above n, rows that are not
+ * strictly increasing and self loops are refused with BEEP_ERR_INVALID_ARG
+ * before any counting work. Work is ordered on cuda_stream (NULL: the legacy
+ * default stream) and the call waits for it: it returns when the count is on
+ * the host. It calls no cudaMalloc, cudaFree or other
  * allocating routine: its only scratch is a file-scope device array of
  * BEEP_NOALLOC_SCRATCH_BYTES. The first call on a device looks up that array's
  * device address; make that first call before any stream capture.
@@ -333,9 +349,10 @@ beep_status beep_serve_destroy(beep_server *s);
  * and are refused with BEEP_ERR_UNSUPPORTED. Roots whose search domain exceeds
  * 1024 vertices keep their bitmap in the scratch array, so the largest domain
  * (a root's neighbours, or its higher-id neighbours for clique-like queries)
- * is limited to 23170 vertices; larger inputs are refused with
- * BEEP_ERR_UNSUPPORTED before any work. The fewer such slices fit, the fewer
- * blocks run. All calls on a device share the scratch array, which keeps the
+ * is limited to BEEP_NOALLOC_MAX_DOMAIN (23168) vertices; larger inputs are
+ * refused with BEEP_ERR_UNSUPPORTED before any counting work; the fewer such
+ * slices fit, the fewer blocks run. A count of BEEP_COUNT_LIMIT or more
+ * returns BEEP_ERR_OVERFLOW. All calls on a device share the scratch array, which keeps the
  * last call's contents (each call clears what must start at zero); calls that
  * overlap on the GPU, from other streams or host threads, race on it. */
 beep_status beep_count_noalloc(int device, void *cuda_stream, int64_t n, int64_t m, const int32_t *d_row_ptr,

@@ -14,7 +14,10 @@ import shutil
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("BEEP_REFERENCE_ROOT", "/root/reference")
+# The reference checkout: BEEP_REFERENCE_ROOT, else a directory named
+# "reference" beside this repository's root.
+REF_ROOT = os.environ.get("BEEP_REFERENCE_ROOT",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 OUT_DIR = os.path.join(HERE, "_ref")
 BINARY = os.path.join(OUT_DIR, "beep_ref")
 

@@ -26,6 +26,8 @@ import beep_b200 as B  # noqa: E402
 from beep_b200 import patterns as P  # noqa: E402
 
 CASES = {
+    # the large config: recorded to show how the reference fails on it
+    "c3": ("c3_rmat_22_28_s11", ("rmat", (22, 28, 0.57, 0.19, 0.19, 11)), [("k5", "sgm")]),
     "c1": ("c1_er_4096_p004_s1", ("er", (4096, 0.004, 1)), [("triangle", "sgc"), ("triangle", "sgm")]),
     "small": ("rmat_9_8_s6", ("rmat", (9, 8, 0.57, 0.19, 0.19, 6)),
               [(p, m) for p in ["triangle", "diamond", "k4", "tailed_triangle", "w5", "k5"] for m in ("sgm", "sgc")]),
@@ -54,6 +56,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--timeout", type=float, default=300)
     ap.add_argument("--cases", default="small,c1,c2")
+    ap.add_argument("--repeat", default="",
+                    help="comma-separated graph/pattern/mode keys to run several times (runs_repeated)")
+    ap.add_argument("--repeats", type=int, default=5)
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)),
                                                   "reference_counts.json"))
     args = ap.parse_args()
@@ -72,17 +77,25 @@ def main():
                 mtx = os.path.join(td, f"{pname}.mtx")
                 B.write_mtx(mtx, P.NAMED[pname])
                 key = f"{gname}/{pname}/{mode}"
-                try:
-                    r = subprocess.run([binary, "-g", bel, "-t", mtx, "-m", mode, "-d", "0"], capture_output=True,
-                                       text=True, timeout=args.timeout)
-                    rec = parse(r.stdout)
-                    rec["returncode"] = r.returncode
-                    if r.returncode != 0:
-                        rec["stderr_tail"] = r.stderr[-300:]
-                except subprocess.TimeoutExpired:
-                    rec = {"count": None, "timeout_s": args.timeout}
-                result["runs"][key] = rec
-                print(key, rec, flush=True)
+                reps = args.repeats if key in args.repeat.split(",") else 1
+                recs = []
+                for _ in range(reps):
+                    try:
+                        r = subprocess.run([binary, "-g", bel, "-t", mtx, "-m", mode, "-d", "0"],
+                                           capture_output=True, text=True, timeout=args.timeout)
+                        rec = parse(r.stdout)
+                        rec["returncode"] = r.returncode
+                        if r.returncode != 0:
+                            rec["stderr_tail"] = r.stderr[-600:]
+                            rec["stdout_tail"] = r.stdout[-600:]
+                    except subprocess.TimeoutExpired:
+                        rec = {"count": None, "timeout_s": args.timeout}
+                    recs.append(rec)
+                    print(key, rec, flush=True)
+                if reps > 1:
+                    result.setdefault("runs_repeated", {})[key] = recs
+                else:
+                    result["runs"][key] = recs[0]
                 with open(args.out, "w") as f:
                     json.dump(result, f, indent=1, sort_keys=True)
 

@@ -1,7 +1,8 @@
-"""The N>1 host path on CPU: two gloo ranks. Roots are independent, so ranks
-that take disjoint root shards (oracle root sampling, stride = world size)
-sum to the full count, and device times are combined as the max over ranks
-(bench.py's helpers)."""
+"""The N>1 host path on CPU: two gloo ranks through bench.py's own sharding
+helper (sharded_counts), with the oracle standing in for beep_count_shard:
+each rank counts the roots whose input id % world == rank, one all-reduce
+sums the per-pattern counts, and device times are combined as the max over
+ranks."""
 import os
 import socket
 
@@ -32,11 +33,17 @@ def _worker(rank, world, port, q):
         from oracle import pyoracle as O
 
         rp, col = B.gen_rmat(11, 8, 0.57, 0.19, 0.19, 5)
-        part = O.count(rp, col, P.DIAMOND, apply_root_cap=False, root_stride=world, root_offset=rank, threads=1)
-        total = bench.sum_over_ranks(int(part["count"]), world)
+        processed = []
+
+        def count_shard(name, shard, nshards):
+            r = O.count(rp, col, P.NAMED[name], apply_root_cap=False, root_mod=nshards, root_rem=shard, threads=1)
+            processed.append(r["roots_processed"])
+            return r["count"]
+
+        totals = bench.sharded_counts(count_shard, ["diamond", "k4"], world, rank)
         slowest = bench.max_over_ranks(float(rank + 1), world)
         bench.barrier(world)
-        q.put((rank, total, slowest, part["roots_processed"]))
+        q.put((rank, totals, slowest, processed[0]))
     finally:
         dist.destroy_process_group()
 
@@ -58,8 +65,9 @@ def test_two_gloo_ranks_shard_roots(built):
         assert p.exitcode == 0
     res = sorted(q.get(timeout=10) for _ in range(world))
     rp, col = gen_rmat(11, 8, 0.57, 0.19, 0.19, 5)
-    full = O.count(rp, col, P.DIAMOND, apply_root_cap=False)
-    for rank, total, slowest, processed in res:
-        assert total == full["count"]
+    full = [O.count(rp, col, P.NAMED[name], apply_root_cap=False) for name in ("diamond", "k4")]
+    for rank, totals, slowest, processed in res:
+        assert totals == [f["count"] for f in full]
         assert slowest == float(world)
-    assert sum(r[3] for r in res) == full["roots"]
+    # the shards partition the roots
+    assert sum(r[3] for r in res) == full[0]["roots_processed"]

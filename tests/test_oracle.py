@@ -135,10 +135,13 @@ def test_oracle_matches_reference_binary(built, golden):
     import os
 
     with open(os.path.join(os.path.dirname(__file__), "golden", "reference_counts.json")) as f:
-        ref = json.load(f)["runs"]
+        data = json.load(f)
+    ref = data["runs"]
     checked = 0
     for key, rec in ref.items():
         gname, pname, mode = key.split("/")
+        if gname not in golden["small"] and gname not in golden["large"]:
+            continue  # a recorded failure (the large config), checked below
         tab = golden["small"] if gname in golden["small"] else golden["large"]
         counts = tab[gname]["counts"][pname]
         unmat = O.plan(P.NAMED[pname], sgc=True)["unmat"]
@@ -148,6 +151,14 @@ def test_oracle_matches_reference_binary(built, golden):
             assert rec["count"] == counts[mode], key
             checked += 1
     assert checked >= 15
+    # The same sgc diamond run repeated on the mid config: the reference's
+    # result changes from run to run (donated subtrees count to full depth
+    # while the main path counts prefixes), always between the two counts.
+    reps = data["runs_repeated"]["c2_rmat_20_3_s7/diamond/sgc"]
+    counts = golden["large"]["c2_rmat_20_3_s7"]["counts"]["diamond"]
+    seen = [r["count"] for r in reps]
+    assert len(seen) >= 5 and len(set(seen)) >= 3, seen
+    assert all(counts["sgc"] <= c <= counts["sgm"] for c in seen), seen
 
 
 def test_non_central_golden_and_closed_forms(built):

@@ -7,6 +7,8 @@ equality, the tolerance of every count test here) on two calls in a row,
 since the shared scratch array keeps the previous call's contents. This file
 is named to be collected last; it passes alone in a fresh process and after
 the other tests."""
+import math
+
 import numpy as np
 import pytest
 
@@ -64,14 +66,88 @@ def test_noalloc_matches_count(name, make):
         g.close()
 
 
-def test_noalloc_refuses_oversized_domain():
-    import torch
-
-    leaves = 30000  # a star: the hub's domain is 30000 > 23170 vertices
+def star(leaves):
+    """Vertex 0 joined to vertices 1..leaves (the hub's domain has `leaves` vertices)."""
     rp = np.zeros(leaves + 2, np.int32)
     rp[1] = leaves
     rp[2:] = leaves + np.arange(1, leaves + 1)
     col = np.concatenate([np.arange(1, leaves + 1), np.zeros(leaves)]).astype(np.int32)
+    return rp, col
+
+
+def test_noalloc_domain_limit_boundary():
+    """The largest domain whose bitmap fits the scratch array is counted; one
+    vertex more is refused before any counting work."""
+    import torch
+
+    leaves = B.NOALLOC_MAX_DOMAIN
+    rp, col = star(leaves)
+    d_rp = torch.from_numpy(rp).cuda()
+    d_col = torch.from_numpy(col).cuda()
+    torch.cuda.synchronize()
+    with B.Context(0) as ctx:
+        g = B.Graph.from_csr(ctx, rp, col)
+        want = B.count(g, P.CLAW, B.SGM)
+        g.close()
+    assert want == math.comb(leaves, 3)
+    for call in range(2):
+        assert B.count_noalloc(0, leaves + 1, len(col), d_rp.data_ptr(), d_col.data_ptr(), P.CLAW, B.SGM) == want
+    rp, col = star(leaves + 1)
+    d_rp = torch.from_numpy(rp).cuda()
+    d_col = torch.from_numpy(col).cuda()
+    torch.cuda.synchronize()
+    with pytest.raises(B.BeepError) as e:
+        B.count_noalloc(0, leaves + 2, len(col), d_rp.data_ptr(), d_col.data_ptr(), P.CLAW, B.SGM)
+    assert e.value.status == B.ERR_UNSUPPORTED
+    assert "scratch" in str(e.value) and str(B.NOALLOC_MAX_DOMAIN) in str(e.value)
+
+
+def test_noalloc_rejects_bad_csr():
+    """A CSR the caller got wrong is refused by the device-side check before
+    any kernel uses an entry as an index: an id at or above n, an unsorted
+    row, a self loop, row pointers beyond m."""
+    import torch
+
+    rp, col = B.gen_erdos_renyi(200, 0.05, 2)
+    n, m = len(rp) - 1, len(col)
+    bad_cases = []
+    c = col.copy()
+    c[rp[5]] = n + 7  # an id out of range
+    bad_cases.append((rp, c))
+    c = col.copy()
+    v = int(np.argmax(np.diff(rp) >= 2))
+    c[rp[v]], c[rp[v] + 1] = c[rp[v] + 1], c[rp[v]]  # an unsorted row
+    bad_cases.append((rp, c))
+    loop = next((u, i) for u in range(n) for i in range(rp[u] + 1, rp[u + 1] - 1) if col[i - 1] < u < col[i + 1])
+    c = col.copy()
+    c[loop[1]] = loop[0]  # a self loop, the row still strictly increasing
+    bad_cases.append((rp, c))
+    r = rp.copy()
+    r[3] = m + 5  # a row pointer beyond m
+    bad_cases.append((r, col))
+    for rpb, cb in bad_cases:
+        d_rp = torch.from_numpy(np.ascontiguousarray(rpb, np.int32)).cuda()
+        d_col = torch.from_numpy(np.ascontiguousarray(cb, np.int32)).cuda()
+        torch.cuda.synchronize()
+        with pytest.raises(B.BeepError) as e:
+            B.count_noalloc(0, n, m, d_rp.data_ptr(), d_col.data_ptr(), P.TRIANGLE, B.SGM)
+        assert e.value.status == B.ERR_INVALID_ARG, str(e.value)
+    # the check leaves the path usable: a valid CSR right after counts as before
+    d_rp = torch.from_numpy(rp).cuda()
+    d_col = torch.from_numpy(col).cuda()
+    torch.cuda.synchronize()
+    with B.Context(0) as ctx:
+        g = B.Graph.from_csr(ctx, rp, col)
+        want = B.count(g, P.TRIANGLE, B.SGM)
+        g.close()
+    assert B.count_noalloc(0, n, m, d_rp.data_ptr(), d_col.data_ptr(), P.TRIANGLE, B.SGM) == want
+
+
+def test_noalloc_refuses_oversized_domain():
+    import torch
+
+    leaves = 30000  # a star: the hub's domain is 30000 > BEEP_NOALLOC_MAX_DOMAIN vertices
+    rp, col = star(leaves)
     d_rp = torch.from_numpy(rp).cuda()
     d_col = torch.from_numpy(col).cuda()
     torch.cuda.synchronize()
