@@ -42,6 +42,8 @@ OPT_NO_VIEW_CACHE = 1 << 2
 OPT_ALG_BYTES = 1 << 3
 OPT_NO_GRAPH = 1 << 4
 OPT_SERIAL_TIERS = 1 << 5
+OPT_WAIT_STALL_TEST = 1 << 6
+OPT_NO_NBHD = 1 << 7
 
 
 class BeepError(RuntimeError):
@@ -78,6 +80,7 @@ class PlanInfo(ctypes.Structure):
         ("restricted", ctypes.c_int32),
         ("central", ctypes.c_int32),
         ("wheel4", ctypes.c_int32),
+        ("nbhd", ctypes.c_int32),
     ]
 
 
@@ -95,7 +98,8 @@ class ServeStats(ctypes.Structure):
     _fields_ = [("requests", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("matches", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
                 ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("span_s", ctypes.c_double),
-                ("max_batch", ctypes.c_double)]
+                ("max_batch", ctypes.c_double), ("refused", ctypes.c_uint64), ("max_inflight_bytes", ctypes.c_uint64),
+                ("budget_bytes", ctypes.c_uint64)]
 
 
 class Stats(ctypes.Structure):
@@ -131,6 +135,10 @@ class Stats(ctypes.Structure):
         ("alg_small_bytes", ctypes.c_uint64),
         ("alg_medium_bytes", ctypes.c_uint64),
         ("alg_large_bytes", ctypes.c_uint64),
+        ("small_tail_ms", ctypes.c_double),
+        ("medium_tail_ms", ctypes.c_double),
+        ("large_tail_ms", ctypes.c_double),
+        ("donated_tasks", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -193,8 +201,8 @@ _SIGNATURES = [
                                          _P(ctypes.c_int32)]),
     ("beep_write_bel", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_int32)]),
     ("beep_convert", ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, _P(ctypes.c_uint64)]),
-    ("beep_batch_autotune", ctypes.c_int, [_vp, ctypes.c_uint32, _P(ctypes.c_uint32 * 4), _P(ctypes.c_double)]),
-    ("beep_batch_set_tiers", ctypes.c_int, [_vp, _P(ctypes.c_uint32 * 4)]),
+    ("beep_batch_autotune", ctypes.c_int, [_vp, ctypes.c_uint32, _P(ctypes.c_uint32 * 5), _P(ctypes.c_double)]),
+    ("beep_batch_set_tiers", ctypes.c_int, [_vp, _P(ctypes.c_uint32 * 5)]),
 ]
 
 
@@ -391,6 +399,7 @@ class Query:
             "restricted": p.restricted,
             "central": p.central,
             "wheel4": p.wheel4,
+            "nbhd": p.nbhd,
         }
 
     def close(self) -> None:
@@ -450,18 +459,19 @@ class Batch:
         out = [int(counts[i]) for i in range(n)]
         return (out, st.as_dict()) if stats else out
 
-    TIER_KEYS = ("tiny_max", "small_max", "med_a_max", "med_max")
+    TIER_KEYS = ("tiny_max", "small_max", "med_a_max", "med_max", "donate_min_iters")
 
     def autotune(self, options: int = 0) -> dict:
         """Pick the tier limits by measurement (beep_batch_autotune); returns
         them with the best counting time in ms."""
-        cfg = (ctypes.c_uint32 * 4)()
+        cfg = (ctypes.c_uint32 * 5)()
         ms = ctypes.c_double()
         _check(lib().beep_batch_autotune(self._h, int(options), ctypes.byref(cfg), ctypes.byref(ms)))
         return {**dict(zip(self.TIER_KEYS, list(cfg))), "count_ms": ms.value}
 
     def set_tiers(self, tiers: dict) -> None:
-        cfg = (ctypes.c_uint32 * 4)(*[int(tiers[k]) for k in self.TIER_KEYS])
+        vals = [int(tiers[k]) for k in self.TIER_KEYS[:4]] + [int(tiers.get("donate_min_iters", 2))]
+        cfg = (ctypes.c_uint32 * 5)(*vals)
         _check(lib().beep_batch_set_tiers(self._h, ctypes.byref(cfg)))
 
     def close(self) -> None:

@@ -445,9 +445,20 @@ beep_status beep_enumerate(beep_ctx *ctx, beep_graph *g, const beep_query *q, ui
     EnumRequest er;
     er.k = k;
     er.d_out = dout.as<int32_t>();
+    // two pairs in one call: the exact count (closed forms allowed) and the
+    // enumerating walk, which stops once k tuples are written
+    std::vector<PairSpec> specs(k > 0 ? 2 : 1);
+    for (auto &ps : specs) {
+        ps.g = &g->impl;
+        ps.plan = p;
+    }
+    if (k > 0)
+        specs[1].en = &er;
+    uint64_t counts[2] = {0, 0};
     beep_stats st;
-    BEEP_TRY(run_count(&ctx->impl, &g->impl, p, 0, k > 0 ? &er : nullptr, &st));
+    BEEP_TRY(run_pairs(&ctx->impl, specs, 0, &st, counts));
     ctx->impl.launches += (uint64_t)st.kernel_launches;
+    st.count = counts[0];
     if (st.count == BEEP_COUNT_OVERFLOW) {
         *n_out = 0;
         if (total_count)
@@ -511,7 +522,7 @@ beep_status beep_batch_run(beep_batch *b, uint32_t options, uint64_t *counts, be
         return fail(BEEP_ERR_INVALID_ARG, "beep_batch_run: bad arguments");
     BEEP_TRY(bind(b->ctx));
     Ctx *ctx = &b->ctx->impl;
-    const uint32_t plan_opts = options & (BEEP_OPT_REFERENCE_ROOT_CAP | BEEP_OPT_NO_VIEW_CACHE);
+    const uint32_t plan_opts = options & (BEEP_OPT_REFERENCE_ROOT_CAP | BEEP_OPT_NO_VIEW_CACHE | BEEP_OPT_NO_NBHD);
     double prep_ms = 0;
     if (!b->plan || b->planned_options != plan_opts) {
         b->plan.reset();
@@ -545,7 +556,7 @@ beep_status beep_batch_set_tiers(beep_batch *b, const beep_tier_cfg *cfg) {
         return fail(BEEP_ERR_INVALID_ARG, "beep_batch_set_tiers: bad arguments");
     BEEP_TRY(bind(b->ctx));
     cudaStreamSynchronize(b->ctx->impl.stream);
-    b->tiers = TierCfg{cfg->tiny_max, cfg->small_max, cfg->med_a_max, cfg->med_max};
+    b->tiers = TierCfg{cfg->tiny_max, cfg->small_max, cfg->med_a_max, cfg->med_max, cfg->donate_min_iters};
     b->plan.reset(); // the next run plans (and captures) with the new limits
     return BEEP_OK;
 }
@@ -570,11 +581,11 @@ beep_status beep_batch_autotune(beep_batch *b, uint32_t options, beep_tier_cfg *
     double best_ms = 0;
     BEEP_TRY(measure(best, &best_ms)); // also builds the views, so later candidates time only the counting
     BEEP_TRY(measure(best, &best_ms));
-    const std::vector<uint32_t> cand[4] = {{0, 8, 16}, {32, 64}, {128, 256}, {512, 1024}};
-    for (int k = 0; k < 4; ++k)
+    const std::vector<uint32_t> cand[5] = {{0, 8, 16}, {32, 64}, {128, 256}, {512, 1024}, {2, 4, 16}};
+    for (int k = 0; k < 5; ++k)
         for (uint32_t val : cand[k]) {
             TierCfg c = best;
-            uint32_t *f[4] = {&c.tiny_max, &c.small_max, &c.med_a_max, &c.med_max};
+            uint32_t *f[5] = {&c.tiny_max, &c.small_max, &c.med_a_max, &c.med_max, &c.donate_min_iters};
             if (*f[k] == val)
                 continue;
             *f[k] = val;
@@ -588,7 +599,7 @@ beep_status beep_batch_autotune(beep_batch *b, uint32_t options, beep_tier_cfg *
     b->tiers = best;
     b->plan.reset();
     if (chosen)
-        *chosen = beep_tier_cfg{best.tiny_max, best.small_max, best.med_a_max, best.med_max};
+        *chosen = beep_tier_cfg{best.tiny_max, best.small_max, best.med_a_max, best.med_max, best.donate_min_iters};
     if (best_count_ms)
         *best_count_ms = best_ms;
     return BEEP_OK;

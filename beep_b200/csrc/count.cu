@@ -94,7 +94,8 @@ __device__ __forceinline__ Lp load_lp(const DevPlan &pl) {
 //     flushes a lane adds fewer than 2^51 that way (2^45 additions take a
 //     lane more than nine hours), so a saturated counter stays below 2^64;
 //   - flushes sum lanes saturating and check the global add for a carry.
-// A pair's counter is two words: the count, then a flag set on overflow.
+// A pair's counter is six words: the walks' count and its overflow flag,
+// then the neighbourhood statistics' positive and negative sums with theirs.
 // ---------------------------------------------------------------------------
 constexpr unsigned long long kCountLimit = BEEP_COUNT_LIMIT;
 static_assert(BEEP_COUNT_LIMIT == 0ull - (1ull << 52), "count limit");
@@ -246,6 +247,12 @@ struct EnumCtx {
     int32_t order[kMaxQ];
 };
 
+// An enumerating walk stops once k tuple slots are reserved (the pair's exact
+// count comes from a counting pair of the same call).
+__device__ __forceinline__ bool enum_full(const EnumCtx &ec) {
+    return ec.en.out != nullptr && *(const volatile unsigned long long *)ec.en.n >= ec.en.k;
+}
+
 __device__ __forceinline__ void emit_bits(const EnumCtx &ec, const uint32_t (&x)[kMaxQ], int P, uint64_t bits,
                                           uint32_t base) {
     // a pair that enumerates nothing may share an enumerating launch
@@ -339,6 +346,10 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
                 cnt += (unsigned long long)__popcll(c);
             } else {
                 while (c) {
+                    if constexpr (ENUM) {
+                        if (enum_full(ec))
+                            return;
+                    }
                     const int b = __ffsll((long long)c) - 1;
                     c &= c - 1;
                     x[P] = (uint32_t)b;
@@ -367,6 +378,10 @@ __device__ __forceinline__ void dfs_thread(const Lp &lp, const uint64_t *rows, u
                 return;
             uint64_t w = cand_word<P, NW>(lp, rows, rlo, D, lo, x, k);
             for (;;) {
+                if constexpr (ENUM) {
+                    if (enum_full(ec))
+                        return;
+                }
                 while (!w) {
                     if (++k >= nw)
                         return;
@@ -402,10 +417,138 @@ struct RowLists {
     uint32_t cap = 0;              // 0: no lists
 };
 
-template <int P, int DEND, bool ENUM, int G = 32, bool LIST = false>
+// ---------------------------------------------------------------------------
+// work donation of the large tier. The reference hands a DFS subtree to an
+// idle block through a ticket queue once the global roots run out
+// (include/queue.cuh:17-56, device_utils.cuh:328-424, sgm_kernelsLD.cuh:
+// 89-106, 135-271), with unbounded spins and a recipient that reads the
+// donor's bitmap while the donor may overwrite it. Here the large tier's rows
+// sit in the arena for the whole launch, so a donated task is just indices:
+// (batch entry, x1, level P, x[2 .. P-1], an iteration range of level P).
+//   - Warps first take the static (root, x1) tasks from the cursor. A warp
+//     that finds it empty claims the next queue slot (head) and waits for it.
+//   - A running warp at a level 2 <= P <= max_level that is not closed-form
+//     checks at every iteration whether slots are claimed but not reserved
+//     (head > tail); if so and at least min_iters iterations remain, it
+//     reserves a slot (tail), writes the upper half of its remaining range
+//     there, publishes it (ready flag after a fence) and keeps the lower half.
+//   - Termination: pending counts reserved donated tasks not yet finished and
+//     static_done the finished static tasks. A waiting warp leaves when every
+//     static task is done and nothing is pending: no task runs, so none can
+//     be donated any more.
+//   - Waits are bounded: a waiting warp that sees no progress (a reservation,
+//     a finished task or a donor's heartbeat) for timeout_ns sets the error
+//     word and returns, so a kernel never spins without end; the host reports
+//     BEEP_ERR_TIMEOUT.
+// ---------------------------------------------------------------------------
+struct DonTask {
+    uint32_t b;          // batch entry (root) of the task
+    uint32_t x1;         // level-1 vertex (domain index)
+    uint32_t level;      // level whose iteration range the task covers
+    uint32_t it_lo, it_hi;
+    uint32_t x[kMaxQ - 2]; // x[2 .. level - 1]
+    uint32_t pad[3];
+};
+static_assert(sizeof(DonTask) == 64, "donated task record");
+
+enum DonCtl : uint32_t {
+    kDonHead = 0,       // slots claimed by waiting warps
+    kDonTail = 1,       // slots reserved by donors
+    kDonPending = 2,    // donated tasks reserved and not finished
+    kDonHeartbeat = 3,  // bumped by running warps that see waiters but cannot donate
+    kDonError = 4,      // 1: a wait ran out
+    kDonCount = 5,      // donations made
+    kDonStaticDone = 6, // static tasks finished
+    kDonDone = 7,       // donated tasks finished
+    kDonWords = 8
+};
+
+struct Don {
+    DonTask *tasks = nullptr;
+    unsigned *ready = nullptr; // cap flags
+    unsigned *ctl = nullptr;   // kDonWords
+    uint32_t cap = 0;          // 0: no donation
+    uint32_t max_level = 0;    // donate at levels 2 .. max_level
+    uint32_t min_iters = 2;    // ... when at least this many iterations remain
+    unsigned long long timeout_ns = 1000000000ull;
+};
+
+__device__ __forceinline__ unsigned ld_volatile(const unsigned *p) { return *(const volatile unsigned *)p; }
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Earliest and latest exit of a launch's warps: exit_t[0] holds the largest
+// complemented time (so one zero fill starts both words), exit_t[1] the
+// largest time. Called by one lane of each warp (or block) as it leaves.
+__device__ __forceinline__ void record_exit(unsigned long long *exit_t) {
+    if (exit_t) {
+        const unsigned long long t = global_ns();
+        atomicMax(exit_t, ~t);
+        atomicMax(exit_t + 1, t);
+    }
+}
+
+// What a donating warp knows about its task: where to donate, and the task's
+// batch entry and level-1 vertex (copied into every task it donates); and
+// when lane 0 last bumped the heartbeat.
+struct DonCtx {
+    const Don *dn = nullptr;
+    uint32_t b = 0, x1 = 0;
+    unsigned long long last_beat = 0;
+};
+
+// Lane 0 of a warp that sees waiting warps but cannot donate shows progress,
+// at most every 100 microseconds.
+__device__ __forceinline__ void heartbeat(DonCtx &dc) {
+    const unsigned long long t = global_ns();
+    if (t - dc.last_beat > 100000ull) {
+        dc.last_beat = t;
+        atomicAdd(&dc.dn->ctl[kDonHeartbeat], 1u);
+    }
+}
+
+// Lane 0 reserves a slot and writes the task [lo, hi) of level P; false when
+// the queue is full (the donor keeps the work).
+template <int P>
+__device__ __forceinline__ bool donate(const DonCtx &dc, const uint32_t (&x)[kMaxQ], uint32_t lo, uint32_t hi,
+                                       int lane) {
+    const Don &dn = *dc.dn;
+    uint32_t s = 0;
+    if (lane == 0) {
+        atomicAdd(&dn.ctl[kDonPending], 1u);
+        s = atomicAdd(&dn.ctl[kDonTail], 1u);
+        if (s < dn.cap) {
+            DonTask *t = dn.tasks + s;
+            t->b = dc.b;
+            t->x1 = dc.x1;
+            t->level = (uint32_t)P;
+            t->it_lo = lo;
+            t->it_hi = hi;
+#pragma unroll
+            for (int q = 2; q < P; ++q)
+                t->x[q - 2] = x[q];
+            __threadfence();
+            atomicExch(&dn.ready[s], 1u);
+            atomicAdd(&dn.ctl[kDonCount], 1u);
+        } else {
+            atomicSub(&dn.ctl[kDonPending], 1u);
+        }
+    }
+    s = __shfl_sync(kFull, s, 0);
+    return s < dn.cap;
+}
+
+template <int P, int DEND, bool ENUM, int G = 32, bool LIST = false, bool DON = false>
 __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint32_t rlo, uint32_t W, uint32_t D,
                                          uint32_t (&x)[kMaxQ], unsigned long long &cnt, int glane, const EnumCtx &ec,
-                                         unsigned gmask = kFull, const RowLists &rl = RowLists()) {
+                                         unsigned gmask = kFull, const RowLists &rl = RowLists(),
+                                         DonCtx *dc = nullptr, uint32_t r_lo = 0,
+                                         uint32_t r_hi = 0xffffffffu) {
+    static_assert(!DON || G == 32, "donation is by whole warps");
     constexpr int LG = G == 32 ? 5 : (G == 16 ? 4 : (G == 8 ? 3 : (G == 4 ? 2 : (G == 2 ? 1 : 0))));
     static_assert((1 << LG) == G, "group size must be a power of two up to 32");
     static_assert(!LIST || G == 32, "row lists are read by whole warps");
@@ -451,7 +594,45 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
             }
         }
     }
+    // a donated task covers part of this level's iterations
+    it0 = max(it0, r_lo);
+    it1 = min(it1, r_hi);
     for (uint32_t it = it0; it < it1; ++it) {
+        if constexpr (ENUM && P < DEND - 1) {
+            unsigned full = glane == 0 ? (unsigned)enum_full(ec) : 0u;
+            full = __shfl_sync(gmask, full, 0, G);
+            if (full)
+                return;
+        }
+        if constexpr (DON && P < DEND - 1) {
+            // below the donation levels: only show progress to waiting warps
+            // (a long subtree must not look like a hang)
+            if (P > (int)dc->dn->max_level && glane == 0) {
+                const unsigned long long t = global_ns();
+                if (t - dc->last_beat > 200000ull) {
+                    dc->last_beat = t;
+                    const unsigned *ctl = dc->dn->ctl;
+                    if (ld_volatile(&ctl[kDonHead]) > ld_volatile(&ctl[kDonTail]))
+                        atomicAdd(&dc->dn->ctl[kDonHeartbeat], 1u);
+                }
+            }
+            // hand the upper half of the remaining iterations to a waiting warp
+            if (!closed && P <= (int)dc->dn->max_level) {
+                unsigned want = 0;
+                if (glane == 0) {
+                    const unsigned *ctl = dc->dn->ctl;
+                    want = ld_volatile(&ctl[kDonHead]) > ld_volatile(&ctl[kDonTail]) && !ld_volatile(&ctl[kDonError]);
+                }
+                want = __shfl_sync(kFull, want, 0);
+                if (want) {
+                    const uint32_t mid = it + 1 + (it1 - it - 1) / 2;
+                    if (it1 - it >= dc->dn->min_iters && donate<P>(*dc, x, mid, it1, glane))
+                        it1 = mid;
+                    else if (glane == 0)
+                        heartbeat(*dc);
+                }
+            }
+        }
         // this lane's word (none when k >= W)
         uint32_t k;
         if (LIST && listed) {
@@ -498,7 +679,7 @@ __device__ __forceinline__ void dfs_warp(const Lp &lp, const uint32_t *bm, uint3
                 if (LIST && listed)
                     kk = __shfl_sync(gmask, k, L, G);
                 x[P] = (kk << 5) + (uint32_t)b;
-                dfs_warp<P + 1, DEND, ENUM, G, LIST>(lp, bm, rlo, W, D, x, cnt, glane, ec, gmask, rl);
+                dfs_warp<P + 1, DEND, ENUM, G, LIST, DON>(lp, bm, rlo, W, D, x, cnt, glane, ec, gmask, rl, dc);
                 bal = __ballot_sync(gmask, w != 0) >> gbase;
                 if constexpr (G < 32)
                     bal &= (1u << G) - 1u;
@@ -684,6 +865,127 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
 }
 
 // ---------------------------------------------------------------------------
+// Row building for a block over a domain of at most kMediumMaxD vertices,
+// through a shared-memory hash of the domain (vertex id -> domain index):
+//   1. per row i: A[i]'s higher-priority list, untrimmed (its two row
+//      pointers and split, one global round trip per row);
+//   2. exclusive prefix of the per-row work;
+//   3. warp w takes the contiguous work range [w * chunk, (w + 1) * chunk),
+//      32 items a step (consecutive lanes read consecutive list entries);
+//      each lane's row advances monotonically instead of being searched per
+//      item. A list entry is looked up in the hash (about two shared loads);
+//      the A entries of a row whose list is far longer than that part of A
+//      (nA * log2(c) * 4 < c) are instead searched in the list.
+// The hash has 2^k >= 2D slots of vertex ids (all ones: empty) with the
+// domain index beside each; multiplicative hashing, linear probing.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kHashEmpty = 0xffffffffu;
+
+__host__ __device__ __forceinline__ uint32_t hash_slots(uint32_t maxD) {
+    uint32_t s = 64;
+    while (s < 2 * maxD)
+        s <<= 1;
+    return s;
+}
+
+__device__ __forceinline__ uint32_t hash_of(uint32_t w, uint32_t hshift) { return (w * 0x9E3779B1u) >> hshift; }
+
+// Fills the hash of A[0, D) (block-wide; the caller syncs before and after).
+__device__ __forceinline__ void hash_build(const uint32_t *A, uint32_t D, uint32_t *hkeys, uint16_t *hidx,
+                                           uint32_t nslots, uint32_t hshift) {
+    for (uint32_t i = threadIdx.x; i < nslots; i += blockDim.x)
+        hkeys[i] = kHashEmpty;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < D; i += blockDim.x) {
+        const uint32_t w = A[i];
+        uint32_t s = hash_of(w, hshift);
+        while (atomicCAS(&hkeys[s], kHashEmpty, w) != kHashEmpty)
+            s = (s + 1) & (nslots - 1);
+        hidx[s] = (uint16_t)i;
+    }
+}
+
+// Domain index of w, or -1.
+__device__ __forceinline__ int hash_find(const uint32_t *hkeys, const uint16_t *hidx, uint32_t nslots,
+                                         uint32_t hshift, uint32_t w) {
+    uint32_t s = hash_of(w, hshift);
+    for (;;) {
+        const uint32_t key = hkeys[s];
+        if (key == w)
+            return (int)hidx[s];
+        if (key == kHashEmpty)
+            return -1;
+        s = (s + 1) & (nslots - 1);
+    }
+}
+
+template <typename SetFn>
+__device__ __forceinline__ void build_rows_hashed(const ViewDev &v, int asc, const uint32_t *A, uint32_t D,
+                                                  uint32_t rlo, uint32_t *s_hb, uint32_t *s_pre, uint32_t *s_len,
+                                                  const uint32_t *hkeys, const uint16_t *hidx, uint32_t nslots,
+                                                  uint32_t hshift, SetFn set) {
+    constexpr uint32_t kByA = 0x80000000u;
+    const uint32_t R = D, tid = threadIdx.x, nthr = blockDim.x;
+    for (uint32_t r = tid; r < R; r += nthr) {
+        uint32_t hb, he, xb, xe, work = 0, len = 0;
+        hd_range(v, asc, A[r], r, D, hb, he, xb, xe);
+        if (asc)
+            xb = max(xb, rlo);
+        else if (r < rlo)
+            xe = 0;
+        if (xb < xe && hb < he) {
+            const uint32_t c = he - hb, nA = xe - xb;
+            len = c;
+            work = c;
+            if (c < kByA && (uint64_t)nA * search_steps(c) * 4 < (uint64_t)c) {
+                len = c | kByA;
+                work = nA;
+            }
+        }
+        s_hb[r] = hb;
+        s_len[r] = len;
+        s_pre[r] = work;
+    }
+    __syncthreads();
+    if (tid < 32)
+        warp_excl_scan(s_pre, R, (int)tid);
+    __syncthreads();
+    const uint32_t T = s_pre[R];
+    const uint32_t nw = nthr >> 5, lane = tid & 31;
+    const uint32_t chunk = ((T + nw - 1) / nw + 31) & ~31u;
+    const uint32_t t_begin = (tid >> 5) * chunk, t_end = min(T, t_begin + chunk);
+    uint32_t r = 0;
+    if (t_begin + lane < t_end) { // the row of this lane's first item: last r with s_pre[r] <= t
+        uint32_t lo = 0, hi = R;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_pre[mid] <= t_begin + lane)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        r = lo;
+    }
+    for (uint32_t t = t_begin + lane; t < t_end; t += 32) {
+        while (s_pre[r + 1] <= t)
+            ++r;
+        const uint32_t len = s_len[r];
+        const uint32_t xb = asc ? max(r + 1, rlo) : 0, xe = asc ? D : r;
+        const uint32_t off = t - s_pre[r];
+        if (len & kByA) {
+            const uint32_t k = xb + off;
+            const uint32_t hb = s_hb[r];
+            if (contains_g(v.col, hb, hb + (len & ~kByA), A[k]))
+                set(r, k);
+        } else {
+            const int k = hash_find(hkeys, hidx, nslots, hshift, v.col[s_hb[r] + off]);
+            if (k >= (int)xb && k < (int)xe)
+                set(r, (uint32_t)k);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // work items. A pair is one (graph view, compiled query); an item is one root
 // of one pair, packed as (pair << 32) | root. One launch per tier serves the
 // items of every pair of a call (the plain count is a call with one pair).
@@ -691,6 +993,8 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
 // Slots after the per-pair counters: adjacency bytes read per tier (3), the
 // algorithmic bytes of the searched roots per tier (3), 2 spare.
 constexpr uint32_t kAux = 8;
+// words of a pair's counter: (count, flag), (statistics plus, flag), (minus, flag)
+constexpr uint32_t kPairWords = 6;
 
 struct PairDev {
     ViewDev v;
@@ -853,7 +1157,8 @@ __device__ __forceinline__ unsigned long long wheel4_warp(const uint32_t *rows, 
 
 template <int DEND, bool ENUM, int G, int MAXD>
 __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(const PairDev *__restrict__ pairs,
-                                                           const uint64_t *__restrict__ items, uint32_t nitems) {
+                                                           const uint64_t *__restrict__ items, uint32_t nitems,
+                                                           unsigned long long *exit_t) {
     constexpr int NG = kSmallWarps * 32 / G; // groups per block
     __shared__ uint64_t s_rows[NG][MAXD];
     __shared__ uint32_t s_A[NG][MAXD];
@@ -949,6 +1254,8 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
     cnt = group_sum<G>(cnt, gmask);
     if (glane == 0)
         flush_count(pr.count, cnt);
+    if (lane == 0)
+        record_exit(exit_t);
 }
 
 // ---------------------------------------------------------------------------
@@ -964,16 +1271,19 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
 template <int DEND, bool ENUM, int G>
 __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 : 2) : 1) k_medium(const PairDev *__restrict__ pairs,
                                                 const uint64_t *__restrict__ items, uint32_t nitems,
-                                                unsigned *cursor, uint32_t maxD) {
+                                                unsigned *cursor, uint32_t maxD, unsigned long long *exit_t) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t s_ri, s_j;
     const int lane = threadIdx.x & 31;
     const uint32_t pad = (maxD + 4) & ~3u;
+    const uint32_t nslots = hash_slots(maxD), hshift = 32u - (uint32_t)__ffs((int)nslots) + 1u;
     uint32_t *A = sm;
     uint32_t *s_hb = sm + pad;
     uint32_t *s_pre = sm + 2 * pad;
     uint32_t *s_len = sm + 3 * pad;
-    uint32_t *rows = sm + 4 * pad;
+    uint32_t *hkeys = sm + 4 * pad;                                 // domain hash: vertex ids ...
+    uint16_t *hidx = reinterpret_cast<uint16_t *>(hkeys + nslots); // ... and their domain indices
+    uint32_t *rows = hkeys + nslots + nslots / 2;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
     EnumCtx ec;
@@ -1012,23 +1322,25 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
             s_j = j0;
         __syncthreads();
         if (rlo < D) { // block-uniform
+            hash_build(A, D, hkeys, hidx, nslots, hshift);
+            __syncthreads();
             if constexpr (G == 0) {
                 unsigned long long *r64 = reinterpret_cast<unsigned long long *>(rows);
-                build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, s_len, threadIdx.x, blockDim.x,
-                                   kFull, [&](uint32_t i, uint32_t k) {
-                                       if (i >= rlo)
-                                           atomicOr(&r64[(size_t)(i - rlo) * kThreadNW + (k >> 6)], 1ull << (k & 63));
-                                       if (k >= rlo)
-                                           atomicOr(&r64[(size_t)(k - rlo) * kThreadNW + (i >> 6)], 1ull << (i & 63));
-                                   });
+                build_rows_hashed(pr.v, pr.asc, A, D, rlo, s_hb, s_pre, s_len, hkeys, hidx, nslots, hshift,
+                                  [&](uint32_t i, uint32_t k) {
+                                      if (i >= rlo)
+                                          atomicOr(&r64[(size_t)(i - rlo) * kThreadNW + (k >> 6)], 1ull << (k & 63));
+                                      if (k >= rlo)
+                                          atomicOr(&r64[(size_t)(k - rlo) * kThreadNW + (i >> 6)], 1ull << (i & 63));
+                                  });
             } else {
-                build_rows_flat<0>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb, s_pre, s_len, threadIdx.x, blockDim.x,
-                                   kFull, [&](uint32_t i, uint32_t k) {
-                                       if (i >= rlo)
-                                           atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
-                                       if (k >= rlo)
-                                           atomicOr(&rows[(size_t)(k - rlo) * W + (i >> 5)], 1u << (i & 31));
-                                   });
+                build_rows_hashed(pr.v, pr.asc, A, D, rlo, s_hb, s_pre, s_len, hkeys, hidx, nslots, hshift,
+                                  [&](uint32_t i, uint32_t k) {
+                                      if (i >= rlo)
+                                          atomicOr(&rows[(size_t)(i - rlo) * W + (k >> 5)], 1u << (k & 31));
+                                      if (k >= rlo)
+                                          atomicOr(&rows[(size_t)(k - rlo) * W + (i >> 5)], 1u << (i & 31));
+                                  });
             }
         }
         __syncthreads();
@@ -1123,6 +1435,8 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
     cnt = warp_sum(cnt);
     if (lane == 0)
         flush_count(pr.count, cnt);
+    if (threadIdx.x == 0)
+        record_exit(exit_t);
 }
 
 // ---------------------------------------------------------------------------
@@ -1137,13 +1451,21 @@ struct Batch {
 };
 
 constexpr uint32_t kRowsPerChunk = 256;
-constexpr int kLargeDfsBlocksPerSm = 8; // k_large_dfs grid: 256-thread blocks per SM
+constexpr int kLargeDfsBlocksPerSm = 8; // k_large_wheel grid: 256-thread blocks per SM
+constexpr uint32_t kDonCap = 1u << 18;   // donated tasks per walk launch (16 MiB of records)
+constexpr uint32_t kMaxDonLaunches = 64; // walk launches of a call with a donation queue
 // Depth slot of a root in the tier lists: its plan's depth, except the large
 // tier's 4-wheel roots, which take slot 2 (no plan has depth 2) and run on
 // k_large_wheel.
 constexpr uint32_t kWheelSlot = 2;
-__host__ __device__ __forceinline__ uint32_t depth_slot(const DevPlan &pl, uint32_t tier) {
-    return (tier == 4 && pl.wheel4) ? kWheelSlot : (uint32_t)pl.dend;
+constexpr int kDepthsConst = 11; // dend 0..10
+// Slots kDepthsConst.. hold the same depths for enumerating pairs, which run
+// in launches of their own (the walk that writes tuples, with no closed
+// forms), so that counting pairs of the same call keep theirs.
+constexpr uint32_t kNbhdSlot = 1; // the large tier's roots of neighbourhood-statistics plans
+__host__ __device__ __forceinline__ uint32_t depth_slot(const DevPlan &pl, uint32_t tier, bool enumerating) {
+    return (enumerating ? (uint32_t)kDepthsConst : 0u) +
+           ((tier == 4 && pl.wheel4) ? kWheelSlot : ((tier == 4 && pl.nbhd) ? kNbhdSlot : (uint32_t)pl.dend));
 }
 constexpr uint32_t kLargeSmemA = 48 * 1024; // domain entries staged in shared memory
 
@@ -1155,9 +1477,18 @@ __host__ __device__ __forceinline__ uint32_t list_cap(uint32_t W) { return W >= 
 // Arena words of one large root: rows [rlo, D) of W = ceil(D / 32) words,
 // then (list_cap(W) > 0) each row's non-zero word count and its list,
 // rounded up to 32 words.
-__host__ __device__ __forceinline__ uint64_t large_root_words(uint32_t D, uint32_t rlo) {
+// Roots of a neighbourhood-statistics plan keep, after their rows and lists,
+// the degree of every domain vertex in the neighbourhood graph (D words,
+// rounded up to even) and its edge count (one u64).
+__host__ __device__ __forceinline__ uint64_t nb_deg_offset(uint32_t D, uint32_t rlo) {
     const uint32_t W = (D + 31) / 32, cap = list_cap(W);
-    return ((uint64_t)(D - rlo) * (W + (cap ? cap + 1 : 0)) + 31) & ~(uint64_t)31;
+    return ((uint64_t)(D - rlo) * (W + (cap ? cap + 1 : 0)) + 1) & ~(uint64_t)1;
+}
+__host__ __device__ __forceinline__ uint64_t nb_edges_offset(uint32_t D, uint32_t rlo) {
+    return nb_deg_offset(D, rlo) + ((uint64_t)(D + 1) & ~(uint64_t)1);
+}
+__host__ __device__ __forceinline__ uint64_t large_root_words(uint32_t D, uint32_t rlo, bool nb = false) {
+    return ((nb ? nb_edges_offset(D, rlo) + 2 : nb_deg_offset(D, rlo)) + 31) & ~(uint64_t)31;
 }
 
 __device__ __forceinline__ uint32_t find_batch(const uint32_t *__restrict__ start, uint32_t nb, uint32_t t) {
@@ -1371,9 +1702,33 @@ __device__ __forceinline__ void wheel4_task(const uint32_t *__restrict__ bm, con
     __syncwarp(); // U back to zero before the warp's next task
 }
 
+// A donated task of level P resumes the walk at that level over its
+// iteration range (the task's x[2 .. P-1] restored first).
+template <int P, int DEND, bool ENUM>
+__device__ __forceinline__ void run_donated(const Lp &lp, const uint32_t *rows, uint32_t rlo, uint32_t W, uint32_t D,
+                                            uint32_t (&x)[kMaxQ], unsigned long long &cnt, int lane,
+                                            const EnumCtx &ec, const RowLists &rl, DonCtx &dc, const DonTask &t) {
+    if constexpr (P < DEND - 1) {
+        if (t.level == (uint32_t)P) {
+#pragma unroll
+            for (int q = 2; q < P; ++q)
+                x[q] = t.x[q - 2];
+            dfs_warp<P, DEND, ENUM, 32, true, true>(lp, rows, rlo, W, D, x, cnt, lane, ec, kFull, rl, &dc, t.it_lo,
+                                                     t.it_hi);
+            return;
+        }
+        run_donated<P + 1, DEND, ENUM>(lp, rows, rlo, W, D, x, cnt, lane, ec, rl, dc, t);
+    }
+}
+
+// The large tier's walks: every warp takes (root, x1) tasks from the cursor,
+// then waits for donated ones (see the donation comment above) until none
+// can come. exit_t (may be null): the earliest and latest warp exit times.
 template <int DEND, bool ENUM>
 __global__ void __launch_bounds__(256, (!ENUM && DEND <= 5) ? 3 : 1) k_large_dfs(const PairDev *__restrict__ pairs, Batch bt,
-                                                                      const uint32_t *arena, unsigned *cursor) {
+                                                                      const uint32_t *arena, unsigned *cursor,
+                                                                      const __grid_constant__ Don dn,
+                                                                      unsigned long long *exit_t) {
     const int lane = threadIdx.x & 31;
     const uint32_t base0 = bt.tstart[0]; // the items' tasks are tstart[0] .. tstart[nb] - 1
     const uint32_t total = bt.tstart[bt.nb] - base0;
@@ -1381,15 +1736,13 @@ __global__ void __launch_bounds__(256, (!ENUM && DEND <= 5) ? 3 : 1) k_large_dfs
     uint32_t cur = 0xffffffffu;
     EnumCtx ec;
     unsigned long long cnt = 0;
-    for (;;) {
-        uint32_t t = 0;
-        if (lane == 0)
-            t = atomicAdd(cursor, 1u);
-        t = __shfl_sync(kFull, t, 0);
-        if (t >= total)
-            break;
-        t += base0;
-        const uint32_t b = find_batch(bt.tstart, bt.nb, t);
+    DonCtx dc;
+    dc.dn = &dn;
+    // pair registers, domain and rows of batch entry b
+    uint32_t D = 0, W = 0, rlo = 0, j0 = 0;
+    const uint32_t *rows = nullptr;
+    RowLists rl;
+    auto setup = [&](uint32_t b) {
         const uint64_t it = bt.item[b];
         const uint32_t p = item_pair(it), r = item_root(it);
         if (p != cur) {
@@ -1402,26 +1755,121 @@ __global__ void __launch_bounds__(256, (!ENUM && DEND <= 5) ? 3 : 1) k_large_dfs
             if constexpr (ENUM)
                 make_ec(ec, pairs[p].en, pairs[p].pl, pr.v);
         }
-        uint32_t beg, D, j0;
+        uint32_t beg;
         pair_domain(pr, r, beg, D, j0);
-        const uint32_t W = (D + 31) >> 5;
+        W = (D + 31) >> 5;
         if constexpr (ENUM) {
             ec.A = pr.v.col + beg;
             ec.root = r;
         }
-        uint32_t x[kMaxQ];
-        x[1] = j0 + (t - bt.tstart[b]);
-        const uint32_t rlo = pair_rlo(pr, D, j0);
-        const uint32_t *rows = arena + bt.off[b];
-        RowLists rl;
+        rlo = pair_rlo(pr, D, j0);
+        rows = arena + bt.off[b];
         rl.cap = list_cap(W);
         rl.nzc = rows + (size_t)(D - rlo) * W;
         rl.nzl = rl.nzc + (D - rlo);
-        dfs_warp<2, DEND, ENUM, 32, true>(pr.lp, rows, rlo, W, D, x, cnt, lane, ec, kFull, rl);
+    };
+    for (;;) {
+        uint32_t t = 0;
+        if (lane == 0)
+            t = atomicAdd(cursor, 1u);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= total)
+            break;
+        t += base0;
+        const uint32_t b = find_batch(bt.tstart, bt.nb, t);
+        setup(b);
+        uint32_t x[kMaxQ];
+        x[1] = j0 + (t - bt.tstart[b]);
+        dc.b = b;
+        dc.x1 = x[1];
+        if (dn.cap)
+            dfs_warp<2, DEND, ENUM, 32, true, true>(pr.lp, rows, rlo, W, D, x, cnt, lane, ec, kFull, rl, &dc);
+        else
+            dfs_warp<2, DEND, ENUM, 32, true>(pr.lp, rows, rlo, W, D, x, cnt, lane, ec, kFull, rl);
+        if (dn.cap && lane == 0) {
+            __threadfence(); // this task's donations are counted before it is
+            atomicAdd(&dn.ctl[kDonStaticDone], 1u);
+        }
+    }
+    while (dn.cap) {
+        // claim the next slot and wait until a donor fills it or no work is left
+        uint32_t st = 0, idx = 0; // st: 1 a task, 2 leave
+        if (lane == 0) {
+            idx = atomicAdd(&dn.ctl[kDonHead], 1u);
+            if (idx >= dn.cap) {
+                st = 2;
+            } else {
+                const unsigned *ctl = dn.ctl;
+                auto progress = [&]() {
+                    return ld_volatile(&ctl[kDonTail]) + ld_volatile(&ctl[kDonHeartbeat]) +
+                           ld_volatile(&ctl[kDonStaticDone]) + ld_volatile(&ctl[kDonDone]);
+                };
+                unsigned seen = progress();
+                unsigned long long t0 = global_ns();
+                unsigned sleep_ns = 32;
+                for (;;) {
+                    if (ld_volatile(&dn.ready[idx])) {
+                        st = 1;
+                        break;
+                    }
+                    if (ld_volatile(&ctl[kDonError])) {
+                        st = 2;
+                        break;
+                    }
+                    if (ld_volatile(&ctl[kDonStaticDone]) >= total) {
+                        __threadfence();
+                        if (ld_volatile(&ctl[kDonPending]) == 0) {
+                            st = 2;
+                            break;
+                        }
+                    }
+                    const unsigned now_p = progress();
+                    const unsigned long long now = global_ns();
+                    if (now_p != seen) {
+                        seen = now_p;
+                        t0 = now;
+                    } else if (now - t0 > dn.timeout_ns) {
+                        atomicExch(&dn.ctl[kDonError], 1u);
+                        st = 2;
+                        break;
+                    }
+                    __nanosleep(sleep_ns);
+                    if (sleep_ns < 2048)
+                        sleep_ns *= 2;
+                }
+            }
+        }
+        st = __shfl_sync(kFull, st, 0);
+        idx = __shfl_sync(kFull, idx, 0);
+        if (st != 1)
+            break;
+        __threadfence();
+        DonTask t;
+        {
+            // written by another SM: read past L1
+            const unsigned *src = reinterpret_cast<const unsigned *>(dn.tasks + idx);
+            unsigned *dst = reinterpret_cast<unsigned *>(&t);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                dst[i] = __ldcg(src + i);
+        }
+        setup(t.b);
+        uint32_t x[kMaxQ];
+        x[1] = t.x1;
+        dc.b = t.b;
+        dc.x1 = t.x1;
+        run_donated<2, DEND, ENUM>(pr.lp, rows, rlo, W, D, x, cnt, lane, ec, rl, dc, t);
+        if (lane == 0) {
+            __threadfence();
+            atomicAdd(&dn.ctl[kDonDone], 1u);
+            atomicSub(&dn.ctl[kDonPending], 1u);
+        }
     }
     cnt = warp_sum(cnt);
     if (lane == 0)
         flush_count(pr.count, cnt);
+    if (lane == 0)
+        record_exit(exit_t);
 }
 
 // The large tier's 4-wheel roots (classified into depth slot kWheelSlot):
@@ -1429,7 +1877,7 @@ __global__ void __launch_bounds__(256, (!ENUM && DEND <= 5) ? 3 : 1) k_large_dfs
 // its own scratch, wstride words at wsc + warp * wstride.
 __global__ void __launch_bounds__(256) k_large_wheel(const PairDev *__restrict__ pairs, Batch bt,
                                                      const uint32_t *arena, unsigned *cursor, uint32_t *wsc,
-                                                     uint32_t wstride) {
+                                                     uint32_t wstride, unsigned long long *exit_t) {
     const int lane = threadIdx.x & 31;
     const uint32_t base0 = bt.tstart[0];
     const uint32_t total = bt.tstart[bt.nb] - base0;
@@ -1469,6 +1917,234 @@ __global__ void __launch_bounds__(256) k_large_wheel(const PairDev *__restrict__
     cnt = warp_sum(cnt);
     if (lane == 0)
         flush_count(pr.count, cnt);
+    if (lane == 0)
+        record_exit(exit_t);
+}
+
+// ---------------------------------------------------------------------------
+// neighbourhood statistics (large tier, counts only)
+// ---------------------------------------------------------------------------
+// A five-vertex central query is a cone over a four-vertex graph H; its count
+// at root v is the number of copies of H in the neighbourhood graph
+// G_v = G[N(v)] whose universal vertices follow v (NbhdForm). For the forms
+// here that number is a sum of per-vertex and per-edge terms of G_v, read off
+// the root's bitmap rows: d_u = |row(u)|, E = sum d_u / 2 and, per edge
+// (u, w), the common neighbours row(u) & row(w). The walk instead enumerates
+// every (x1, x2, x3) prefix: on a hub of degree 10^5 that is ~10^13 prefixes,
+// against ~10^8 edge terms here.
+//
+// k_large_nbdeg: d_u of every row and E of every root of the batch whose plan
+// has a form (a warp per row, blocks over 256-row chunks).
+__global__ void __launch_bounds__(256) k_large_nbdeg(const PairDev *__restrict__ pairs, Batch bt, uint32_t *arena) {
+    const uint32_t total = bt.cstart[bt.nb];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint32_t b = find_batch(bt.cstart, bt.nb, c);
+        const uint64_t it = bt.item[b];
+        if (pairs[item_pair(it)].pl.nbhd == kNbNone)
+            continue;
+        PairRegs pr;
+        load_pair(pairs, item_pair(it), pr);
+        uint32_t beg, D, j0;
+        pair_domain(pr, item_root(it), beg, D, j0);
+        const uint32_t W = (D + 31) >> 5;
+        uint32_t *base = arena + bt.off[b]; // rows of the whole domain (rlo = 0)
+        uint32_t *deg = base + nb_deg_offset(D, 0);
+        unsigned long long *E2 = reinterpret_cast<unsigned long long *>(base + nb_edges_offset(D, 0));
+        const uint32_t i0 = (c - bt.cstart[b]) * kRowsPerChunk, i1 = min(D, i0 + kRowsPerChunk);
+        unsigned long long sum = 0;
+        for (uint32_t i = i0 + warp; i < i1; i += nwarps) {
+            const uint32_t *row = base + (size_t)i * W;
+            uint32_t d = 0;
+            for (uint32_t k = lane; k < W; k += 32)
+                d += (uint32_t)__popc(row[k]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                d += __shfl_xor_sync(kFull, d, o);
+            if (lane == 0) {
+                deg[i] = d;
+                sum += d;
+            }
+        }
+        if (lane == 0 && sum)
+            atomicAdd(E2, sum); // twice the edges: E = E2 / 2
+    }
+}
+
+// |row(a) & row(b)| over the shorter of a's word list (al, na) and b's own
+// list; with above, only the bits after domain index lo.
+__device__ __forceinline__ uint32_t common_count(const uint32_t *ra, const uint32_t *rb, const uint32_t *al,
+                                                 uint32_t na, const RowLists &rl, uint32_t b, bool above,
+                                                 uint32_t lo) {
+    const uint32_t nbw = rl.cap ? rl.nzc[b] : 0xffffffffu;
+    const bool use_b = nbw <= rl.cap && nbw < na;
+    const uint32_t *lst = use_b ? rl.nzl + (size_t)b * rl.cap : al;
+    const uint32_t n = use_b ? nbw : na;
+    const uint32_t lw = lo >> 5, lmask = ~((2u << (lo & 31)) - 1u); // bits of word lw above lo
+    uint32_t s = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t e = lst[i];
+        if (above && e < lw)
+            continue;
+        uint32_t w = ra[e] & rb[e];
+        if (above && e == lw)
+            w &= lmask;
+        s += (uint32_t)__popc(w);
+    }
+    return s;
+}
+
+__device__ __forceinline__ unsigned long long binom2(unsigned long long x) { return x * (x - (x ? 1 : 0)) / 2; }
+
+// 128-bit product saturated to the count limit.
+__device__ __forceinline__ unsigned long long sat_mul(unsigned long long a, unsigned long long b) {
+    const unsigned __int128 p = (unsigned __int128)a * b;
+    return p >= (unsigned __int128)kCountLimit ? kCountLimit : (unsigned long long)p;
+}
+
+// Task (root, u): u's terms of the root's form, into plus / minus (lane
+// sums). la: W words of per-warp scratch for u's word list when its row has
+// none.
+__device__ __forceinline__ void nbhd_task(int form, const uint32_t *__restrict__ bm, const RowLists &rl,
+                                          const uint32_t *__restrict__ deg, unsigned long long E, uint32_t W,
+                                          uint32_t D, uint32_t u, bool first, uint32_t *la, int lane,
+                                          unsigned long long &plus, unsigned long long &minus) {
+    const unsigned lt = (1u << lane) - 1u;
+    const unsigned long long du = deg[u], rest = D >= 3 ? D - 3 : 0;
+    if (form == kNbWedgeIso) {
+        if (lane == 0)
+            plus = sat_add(plus, sat_mul(binom2(du), rest));
+        return;
+    }
+    if (form == kNbTwoEdges) {
+        if (lane == 0) {
+            if (first) { // C(E, 2), exact through 128 bits
+                const unsigned __int128 c2 = ((unsigned __int128)E * (E - (E ? 1 : 0))) / 2;
+                plus = sat_add(plus, c2 >= (unsigned __int128)kCountLimit ? kCountLimit : (unsigned long long)c2);
+            }
+            minus = sat_add(minus, binom2(du));
+        }
+        return;
+    }
+    // the other forms sum over the edges (u, w): w after u, or every w (paw)
+    const bool all_w = form == kNbPaw;
+    const uint32_t *ru = bm + (size_t)u * W;
+    const uint32_t uw = u >> 5;
+    const uint32_t *al = la;
+    uint32_t na = 0;
+    if (rl.cap && rl.nzc[u] <= rl.cap) {
+        al = rl.nzl + (size_t)u * rl.cap;
+        na = rl.nzc[u];
+    } else {
+        for (uint32_t k0 = 0; k0 < W; k0 += 32) {
+            const uint32_t k = k0 + (uint32_t)lane;
+            const uint32_t w = k < W ? ru[k] : 0u;
+            const unsigned bal = __ballot_sync(kFull, w != 0);
+            if (w)
+                la[na + (uint32_t)__popc(bal & lt)] = k;
+            na += (uint32_t)__popc(bal);
+        }
+        __syncwarp();
+    }
+    unsigned long long tri = 0; // paw: triangles at u (lane part)
+    for (uint32_t t0 = 0; t0 < na; t0 += 32) {
+        uint32_t bits = 0, k = 0;
+        if (t0 + (uint32_t)lane < na) {
+            k = al[t0 + lane];
+            bits = ru[k];
+            if (!all_w)
+                bits = k < uw ? 0u : (k == uw ? (bits & ~((2u << (u & 31)) - 1u)) : bits);
+        }
+        while (bits) {
+            const uint32_t w = (k << 5) + (uint32_t)(__ffs(bits) - 1);
+            bits &= bits - 1;
+            const uint32_t *rw = bm + (size_t)w * W;
+            switch (form) {
+            case kNbTriIso: // triangles (u < w < x) once, times the isolated vertex's choices
+                plus = sat_add(plus, sat_mul(common_count(ru, rw, al, na, rl, w, true, w), rest));
+                break;
+            case kNbPath4: // paths x - u - w - y, minus the closed ones (x = y): 3T
+                plus = sat_add(plus, (du - 1) * ((unsigned long long)deg[w] - 1));
+                minus = sat_add(minus, common_count(ru, rw, al, na, rl, w, false, 0));
+                break;
+            case kNbPaw: // triangles (u, w, x) with x after w: each once
+                tri += common_count(ru, rw, al, na, rl, w, true, w);
+                break;
+            case kNbDiamond: { // C(common neighbours, 2) of the edge (u, w)
+                const unsigned long long c = common_count(ru, rw, al, na, rl, w, false, 0);
+                plus = sat_add(plus, binom2(c));
+                break;
+            }
+            default:
+                break;
+            }
+        }
+    }
+    if (form == kNbPaw) {
+        tri = warp_sum(tri);
+        if (lane == 0 && du >= 2)
+            plus = sat_add(plus, sat_mul(tri, du - 2));
+    }
+    __syncwarp(); // la reused by the warp's next task
+}
+
+// The large tier's roots of neighbourhood-statistics plans (depth slot
+// kNbhdSlot): every warp takes (root, u) tasks from the cursor. The task of
+// the root's first domain vertex also adds the root-level term.
+__global__ void __launch_bounds__(256) k_large_nbhd(const PairDev *__restrict__ pairs, Batch bt,
+                                                    const uint32_t *arena, unsigned *cursor, uint32_t *wsc,
+                                                    uint32_t wstride, unsigned long long *exit_t) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t base0 = bt.tstart[0];
+    const uint32_t total = bt.tstart[bt.nb] - base0;
+    uint32_t *la = wsc + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * wstride;
+    PairRegs pr;
+    uint32_t cur = 0xffffffffu;
+    int form = kNbNone;
+    unsigned long long plus = 0, minus = 0;
+    for (;;) {
+        uint32_t t = 0;
+        if (lane == 0)
+            t = atomicAdd(cursor, 1u);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= total)
+            break;
+        t += base0;
+        const uint32_t b = find_batch(bt.tstart, bt.nb, t);
+        const uint64_t it = bt.item[b];
+        const uint32_t p = item_pair(it), r = item_root(it);
+        if (p != cur) {
+            plus = warp_sum(plus);
+            minus = warp_sum(minus);
+            if (lane == 0) {
+                flush_count(pr.count + 2, plus);
+                flush_count(pr.count + 4, minus);
+            }
+            plus = minus = 0;
+            cur = p;
+            load_pair(pairs, p, pr);
+            form = pairs[p].pl.nbhd;
+        }
+        uint32_t beg, D, j0;
+        pair_domain(pr, r, beg, D, j0);
+        const uint32_t W = (D + 31) >> 5;
+        const uint32_t *rows = arena + bt.off[b]; // rows of the whole domain: rlo == 0
+        RowLists rl;
+        rl.cap = list_cap(W);
+        rl.nzc = rows + (size_t)D * W;
+        rl.nzl = rl.nzc + D;
+        const uint32_t *deg = rows + nb_deg_offset(D, 0);
+        const unsigned long long E = *reinterpret_cast<const unsigned long long *>(rows + nb_edges_offset(D, 0)) / 2;
+        const uint32_t u = j0 + (t - bt.tstart[b]);
+        nbhd_task(form, rows, rl, deg, E, W, D, u, t == bt.tstart[b], la, lane, plus, minus);
+    }
+    plus = warp_sum(plus);
+    minus = warp_sum(minus);
+    if (lane == 0) {
+        flush_count(pr.count + 2, plus);
+        flush_count(pr.count + 4, minus);
+        record_exit(exit_t);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1544,6 +2220,10 @@ __device__ void gen_walk(const GenRegs &g, uint32_t (&x)[kMaxQ], unsigned long l
                 }
             }
         for (uint32_t k = lower_bound_g(g.v.col, db, de, lo); k < de; ++k) {
+            if constexpr (ENUM) {
+                if (g.en.out && *(const volatile unsigned long long *)g.en.n >= g.en.k)
+                    return;
+            }
             const uint32_t w = g.v.col[k];
             bool ok = true;
 #pragma unroll
@@ -1620,7 +2300,8 @@ __global__ void k_gen_tasks(const uint32_t *__restrict__ D, const uint32_t *__re
 // ---------------------------------------------------------------------------
 constexpr int kTiers = 5;   // 1 small (D <= 64), 2 medium (<= 256), 3 medium (<= 1024), 4 large,
                             // 5 list walker (queries without a central vertex)
-constexpr int kDepths = 11; // dend 0..10
+constexpr int kDepths = kDepthsConst;
+constexpr int kSlots = 2 * kDepths; // depth slots: counting pairs, then enumerating pairs
 
 __device__ __forceinline__ uint32_t find_pair(const uint64_t *__restrict__ offs, uint32_t npairs, uint64_t t) {
     uint32_t lo = 0, hi = npairs;
@@ -1639,11 +2320,11 @@ __device__ __forceinline__ uint32_t find_pair(const uint64_t *__restrict__ offs,
 __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__restrict__ offs, uint32_t npairs,
                            uint64_t N, TierCfg cfg, uint8_t *tier, uint32_t *dom, unsigned *tier_max,
                            unsigned *tier_depth, unsigned *tiny_depth, unsigned long long *large_words) {
-    __shared__ unsigned s_hist[kTiers * kDepths];
-    __shared__ unsigned s_tiny[kDepths];
-    for (int i = threadIdx.x; i < kTiers * kDepths; i += blockDim.x)
+    __shared__ unsigned s_hist[kTiers * kSlots];
+    __shared__ unsigned s_tiny[kSlots];
+    for (int i = threadIdx.x; i < kTiers * kSlots; i += blockDim.x)
         s_hist[i] = 0;
-    for (int i = threadIdx.x; i < kDepths; i += blockDim.x)
+    for (int i = threadIdx.x; i < kSlots; i += blockDim.x)
         s_tiny[i] = 0;
     __syncthreads();
     uint32_t mx[kTiers] = {0, 0, 0, 0, 0};
@@ -1679,13 +2360,14 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
         dom[t] = D;
         if (tc == 4) {
             const uint32_t rn = pd.pl.rows_needed, rlo = rn == 2 ? 0u : (rn == 1 ? j0 : D);
-            atomicAdd(large_words, (unsigned long long)large_root_words(D, rlo));
+            atomicAdd(large_words, (unsigned long long)large_root_words(D, rlo, pd.pl.nbhd != kNbNone));
         }
         if (tc) {
             mx[tc - 1] = max(mx[tc - 1], D);
-            atomicAdd(&s_hist[(tc - 1) * kDepths + depth_slot(pd.pl, tc)], 1u);
+            const uint32_t slot = depth_slot(pd.pl, tc, pd.en.out != nullptr);
+            atomicAdd(&s_hist[(tc - 1) * kSlots + slot], 1u);
             if (tc == 1 && D <= cfg.tiny_max)
-                atomicAdd(&s_tiny[pd.pl.dend], 1u);
+                atomicAdd(&s_tiny[slot], 1u);
         }
     }
 #pragma unroll
@@ -1695,16 +2377,16 @@ __global__ void k_classify(const PairDev *__restrict__ pairs, const uint64_t *__
             atomicMax(&tier_max[k], m);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kTiers * kDepths; i += blockDim.x)
+    for (int i = threadIdx.x; i < kTiers * kSlots; i += blockDim.x)
         if (s_hist[i])
             atomicAdd(&tier_depth[i], s_hist[i]);
-    for (int i = threadIdx.x; i < kDepths; i += blockDim.x)
+    for (int i = threadIdx.x; i < kSlots; i += blockDim.x)
         if (s_tiny[i])
             atomicAdd(&tiny_depth[i], s_tiny[i]);
 }
 
 // Sort keys of every flattened vertex for all item lists at once:
-// (tier, depth, domain order) -- small roots by domain ascending, medium and
+// (tier, depth slot, domain order) -- small roots by domain ascending, medium and
 // large ones by domain descending (heaviest first), list-walker roots by
 // depth only; non-roots last.
 __global__ void k_list_keys(const uint8_t *__restrict__ tier, const uint32_t *__restrict__ dom,
@@ -1716,10 +2398,10 @@ __global__ void k_list_keys(const uint8_t *__restrict__ tier, const uint32_t *__
         uint32_t key = 0xffffffffu;
         if (tc) {
             const uint32_t p = find_pair(offs, npairs, t);
-            const uint32_t dend = depth_slot(pairs[p].pl, tc);
+            const uint32_t slot = depth_slot(pairs[p].pl, tc, pairs[p].en.out != nullptr);
             const uint32_t d = min(dom[t], kDomMask);
             const uint32_t dk = tc == 1 ? d : (tc == 5 ? 0u : kDomMask - d);
-            key = ((tc - 1) << 28) | (dend << 24) | dk;
+            key = ((tc - 1) << 29) | (slot << 24) | dk;
         }
         keys[t] = key;
         vals[t] = (uint32_t)t;
@@ -1743,9 +2425,10 @@ __global__ void k_large_meta(const PairDev *__restrict__ pairs, const uint64_t *
                              unsigned long long *words, uint32_t *chunks, uint32_t *tasks) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nl; i += gridDim.x * blockDim.x) {
         const uint32_t D = D_in[i], j0 = j0_in[i];
-        const uint32_t rn = (uint32_t)pairs[item_pair(items[i])].pl.rows_needed;
+        const DevPlan &pl = pairs[item_pair(items[i])].pl;
+        const uint32_t rn = (uint32_t)pl.rows_needed;
         const uint32_t rlo = rn == 2 ? 0u : (rn == 1 ? j0 : D);
-        words[i] = large_root_words(D, rlo);
+        words[i] = large_root_words(D, rlo, pl.nbhd != kNbNone);
         chunks[i] = (D + kRowsPerChunk - 1) / kRowsPerChunk;
         tasks[i] = D - j0;
     }
@@ -1824,13 +2507,13 @@ __global__ void k_alg_bytes(const PairDev *__restrict__ pairs, const uint64_t *_
 
 template <bool ENUM>
 beep_status launch_small(int dend, int group, int grid, cudaStream_t s, const PairDev *pairs, const uint64_t *items,
-                         uint32_t n) {
+                         uint32_t n, unsigned long long *exit_t) {
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
         if (group == 8)                                                                                            \
-            k_small<D, ENUM, 8, kTinyMaxD><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n);                      \
+            k_small<D, ENUM, 8, kTinyMaxD><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n, exit_t);              \
         else                                                                                                       \
-            k_small<D, ENUM, 32, kSmallMaxD><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n);                    \
+            k_small<D, ENUM, 32, kSmallMaxD><<<grid, kSmallWarps * 32, 0, s>>>(pairs, items, n, exit_t);            \
         break;
     BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
 #undef BEEP_CASE
@@ -1859,14 +2542,28 @@ template <int D, bool ENUM> beep_status set_medium_attr(size_t smem) {
 
 template <bool ENUM>
 beep_status launch_large_dfs(int dend, int grid, cudaStream_t s, const PairDev *pairs, const Batch &bt,
-                             const uint32_t *arena, unsigned *cursor) {
+                             const uint32_t *arena, unsigned *cursor, const Don &dn, unsigned long long *exit_t) {
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
-        k_large_dfs<D, ENUM><<<grid, 256, 0, s>>>(pairs, bt, arena, cursor);                                        \
+        k_large_dfs<D, ENUM><<<grid, 256, 0, s>>>(pairs, bt, arena, cursor, dn, exit_t);                            \
         break;
     BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
 #undef BEEP_CASE
     BEEP_CUDA_TRY(cudaGetLastError());
+    return BEEP_OK;
+}
+
+// Blocks of k_large_dfs that are resident on one SM at once (the persistent
+// grid is that many per SM).
+template <bool ENUM> beep_status large_dfs_blocks_per_sm(int dend, int *out) {
+    int nb = 1;
+#define BEEP_CASE(D)                                                                                               \
+    case D:                                                                                                        \
+        BEEP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_large_dfs<D, ENUM>, 256, 0));           \
+        break;
+    BEEP_DEPTH_SWITCH(dend, BEEP_CASE)
+#undef BEEP_CASE
+    *out = std::max(nb, 1);
     return BEEP_OK;
 }
 
@@ -1884,7 +2581,8 @@ beep_status launch_large_dfs(int dend, int grid, cudaStream_t s, const PairDev *
 // captured once into a CUDA graph (capture_plan) and relaunched.
 // ---------------------------------------------------------------------------
 struct LaunchRec {
-    enum Kind { kSmall, kMedium, kLargeRows, kLargeLists, kLargeDfs, kLargeWheel, kGeneral, kMemset } kind;
+    enum Kind { kSmall, kMedium, kLargeRows, kLargeLists, kLargeDfs, kLargeWheel, kGeneral, kMemset, kLargeNbDeg,
+                kLargeNbhd } kind;
     const uint32_t *tstart = nullptr; // list walker: task prefix of the items
     int dend = 0, grid = 0, block = 0;
     int group = 32; // small tier: lanes per root
@@ -1898,7 +2596,21 @@ struct LaunchRec {
     double *sink = nullptr;   // stats field this launch's time adds to
     uint32_t *wsc = nullptr;  // large tier: 4-wheel scratch, wstride words a warp
     uint32_t wstride = 0;
+    bool enumerate = false;   // the launch writes tuples (its pairs' walks have no closed forms)
+    Don don{};                // large-tier walks: the donation queue (cap 0: none)
+    int tail_slot = -1;       // stats tail this launch's exit spread counts to (0 small, 1 medium, 2 large)
 };
+
+// The degree pass of the neighbourhood-statistics roots a kLargeRows record builds.
+static LaunchRec nbdeg_rec(const LaunchRec &rows) {
+    LaunchRec r = rows;
+    r.kind = LaunchRec::kLargeNbDeg;
+    r.block = 256;
+    r.smem = 0;
+    r.grid = rows.grid * 4;
+    r.cursor = nullptr;
+    return r;
+}
 
 // The list pass over the rows a kLargeRows record builds.
 static LaunchRec lists_rec(const LaunchRec &rows) {
@@ -1931,6 +2643,20 @@ struct LaunchPlan {
     bool own_h_counts = false;
     std::vector<LaunchRec> recs;
     bool enumerate = false;
+    // donation queue of the large tier (shared by its walk launches, which run
+    // one after another on one stream) and one control block per walk launch
+    DonTask *d_don_tasks = nullptr;
+    unsigned *d_don_ready = nullptr;
+    uint32_t don_cap = 0;
+    unsigned *d_don_ctl = nullptr; // kDonWords per walk launch
+    uint32_t ndon = 0;
+    // earliest and latest warp exit of every launch (with BEEP_OPT_TIMING)
+    unsigned long long *d_exit = nullptr;
+    uint32_t nexit = 0;
+    // host words after the pair counts and byte counters: donation control
+    // blocks (as u32), then exit times
+    size_t tel_words() const { return (size_t)ndon * kDonWords / 2 + 2 * (size_t)nexit; }
+    size_t host_words() const { return kPairWords * (size_t)np + kAux + tel_words(); }
     beep_stats st{};
     cudaGraphExec_t exec = nullptr;
     ~LaunchPlan() {
@@ -1957,10 +2683,15 @@ struct LaunchPlan {
 
 void LaunchPlanDeleter::operator()(LaunchPlan *p) const { delete p; }
 
-// Pair i's count after the read-back: BEEP_COUNT_OVERFLOW when its overflow
-// flag is set.
+// Pair i's count after the read-back: the walks' count plus the
+// neighbourhood statistics' sums; BEEP_COUNT_OVERFLOW when a flag is set or
+// the total reaches the limit.
 static uint64_t pair_result(const LaunchPlan *lp, uint32_t i) {
-    return lp->h_counts[2 * (size_t)i + 1] ? BEEP_COUNT_OVERFLOW : lp->h_counts[2 * (size_t)i];
+    const unsigned long long *c = lp->h_counts + kPairWords * (size_t)i;
+    if (c[1] || c[3] || c[5] || c[2] < c[4])
+        return BEEP_COUNT_OVERFLOW;
+    const uint64_t st = c[2] - c[4], v = c[0] + st;
+    return (v < c[0] || v >= BEEP_COUNT_LIMIT) ? BEEP_COUNT_OVERFLOW : v;
 }
 
 beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out,
@@ -2019,11 +2750,11 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     const uint32_t np = (uint32_t)hp.size();
     lp->np = np;
     tr.mark("views");
-    BEEP_TRY(ctx->host_results(2 * (size_t)np + kAux, &lp->h_counts));
-    BEEP_TRY(lp->alloc(lp->d_counts, 3 * (size_t)np + kAux));
+    BEEP_TRY(lp->alloc(lp->d_counts, (kPairWords + 1) * (size_t)np + kAux));
     lp->ncursors = 64;
     BEEP_TRY(lp->alloc(lp->d_cursors, lp->ncursors));
     if (np == 0) {
+        BEEP_TRY(ctx->host_results(lp->host_words(), &lp->h_counts));
         *out = std::move(lp);
         return BEEP_OK;
     }
@@ -2032,10 +2763,14 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         return fail(BEEP_ERR_UNSUPPORTED, "more than 2^32 vertices in one call");
     lp->N = N;
     for (uint32_t i = 0; i < np; ++i) {
-        hp[i].count = lp->d_counts + 2 * (size_t)i;
-        hp[i].en.n = lp->d_counts + 2 * (size_t)np + i; // every pair has a valid tuple counter (k = 0: none written)
-        if (lp->enumerate)
-            hp[i].pl.wheel4 = 0; // the closed form counts; enumeration walks every match
+        hp[i].count = lp->d_counts + kPairWords * (size_t)i;
+        hp[i].en.n = lp->d_counts + kPairWords * (size_t)np + i; // every pair has a tuple counter (k = 0: none written)
+        if (hp[i].en.out) { // the closed forms count; enumeration walks the matches
+            hp[i].pl.wheel4 = 0;
+            hp[i].pl.nbhd = kNbNone;
+        }
+        if (options & BEEP_OPT_NO_NBHD)
+            hp[i].pl.nbhd = kNbNone;
     }
     BEEP_TRY(lp->alloc(lp->d_pairs, np));
     BEEP_TRY(lp->alloc(lp->d_offs, np + 1));
@@ -2051,32 +2786,34 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     BEEP_CUDA_TRY(cudaMemcpyAsync(lp->d_offs, offs.data(), (np + 1) * 8, cudaMemcpyHostToDevice, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(d_misc, 0, 256 * 4, s));
     const int gv = std::max(1, (int)std::min<uint64_t>((N + 255) / 256, (uint64_t)ctx->num_sms * 32));
-    // d_misc: [0, 8) largest domain per tier, [8, 8 + kTiers * kDepths) roots
-    // per (tier, depth), [64, 64 + kDepths) tiny small-tier roots per depth,
-    // [84, 86) arena words of the large tier (u64)
-    static_assert(8 + kTiers * kDepths <= 64, "d_misc layout");
+    // d_misc: [0, 8) largest domain per tier, [8, 8 + kTiers * kSlots) roots
+    // per (tier, depth slot), [120, 120 + kSlots) tiny small-tier roots per
+    // slot, [144, 146) arena words of the large tier (u64)
+    constexpr int kMiscSlots = 8, kMiscTiny = 120, kMiscLarge = 144;
+    static_assert(kMiscSlots + kTiers * kSlots <= kMiscTiny && kMiscTiny + kSlots <= kMiscLarge, "d_misc layout");
     TierCfg cfg = tiers;
     cfg.tiny_max = std::min<uint32_t>(cfg.tiny_max, kTinyMaxD);
     cfg.small_max = std::min<uint32_t>(cfg.small_max, kSmallMaxD);
     cfg.med_a_max = std::min<uint32_t>(cfg.med_a_max, kMediumAMaxD);
     cfg.med_max = std::min<uint32_t>(cfg.med_max, kMediumMaxD);
-    k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, cfg, lp->d_tier, d_dom, d_misc, d_misc + 8,
-                                  d_misc + 64, reinterpret_cast<unsigned long long *>(d_misc + 84));
+    k_classify<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, np, N, cfg, lp->d_tier, d_dom, d_misc,
+                                  d_misc + kMiscSlots, d_misc + kMiscTiny,
+                                  reinterpret_cast<unsigned long long *>(d_misc + kMiscLarge));
     BEEP_CUDA_TRY(cudaGetLastError());
     st.kernel_launches += 1;
-    unsigned h_misc[88];
+    unsigned h_misc[kMiscLarge + 2];
     BEEP_CUDA_TRY(cudaMemcpyAsync(h_misc, d_misc, sizeof(h_misc), cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     const unsigned *tier_max = h_misc;
-    const unsigned *tier_depth = h_misc + 8;
-    const unsigned *tiny_depth = h_misc + 64;
+    const unsigned *tier_depth = h_misc + kMiscSlots; // [tier * kSlots + slot]
+    const unsigned *tiny_depth = h_misc + kMiscTiny;  // [slot]
     uint64_t large_words = 0;
-    std::memcpy(&large_words, h_misc + 84, 8);
+    std::memcpy(&large_words, h_misc + kMiscLarge, 8);
     uint32_t tier_n[kTiers];
     for (int k = 0; k < kTiers; ++k) {
         tier_n[k] = 0;
-        for (int d = 0; d < kDepths; ++d)
-            tier_n[k] += tier_depth[k * kDepths + d];
+        for (int d = 0; d < kSlots; ++d)
+            tier_n[k] += tier_depth[k * kSlots + d];
     }
     st.roots_small = tier_n[0];
     st.roots_medium = (int64_t)tier_n[1] + tier_n[2];
@@ -2086,6 +2823,43 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     tr.mark("classify");
     uint32_t next_cursor = 0;
     auto cursor = [&]() -> unsigned * { return lp->d_cursors + (next_cursor++ % lp->ncursors); };
+    // a walk launch of the large tier: a persistent grid of resident blocks,
+    // and (for k_large_dfs) the donation queue, whose ready flags are cleared
+    // before the launch
+    auto push_walk = [&](LaunchRec ld) -> beep_status {
+        ld.tail_slot = 2;
+        if (ld.kind == LaunchRec::kLargeDfs) {
+            int per_sm = 1;
+            if (ld.enumerate)
+                BEEP_TRY(large_dfs_blocks_per_sm<true>(ld.dend, &per_sm));
+            else
+                BEEP_TRY(large_dfs_blocks_per_sm<false>(ld.dend, &per_sm));
+            ld.grid = ctx->num_sms * per_sm;
+            if (!lp->d_don_tasks) {
+                lp->don_cap = kDonCap;
+                BEEP_TRY(lp->alloc(lp->d_don_tasks, lp->don_cap));
+                BEEP_TRY(lp->alloc(lp->d_don_ready, lp->don_cap));
+                BEEP_TRY(lp->alloc(lp->d_don_ctl, (size_t)kDonWords * kMaxDonLaunches));
+            }
+            if (lp->ndon < kMaxDonLaunches && tiers.donate_min_iters >= 2) {
+                Don &dn = ld.don;
+                dn.tasks = lp->d_don_tasks;
+                dn.ready = lp->d_don_ready;
+                dn.ctl = lp->d_don_ctl + (size_t)kDonWords * lp->ndon++;
+                dn.cap = lp->don_cap;
+                dn.max_level = (uint32_t)(ld.dend + 2) / 2; // levels up to ceil((K + 1) / 2)
+                dn.min_iters = tiers.donate_min_iters;
+                dn.timeout_ns = (unsigned long long)(ctx->wait_timeout_ms * 1e6);
+                LaunchRec ms;
+                ms.kind = LaunchRec::kMemset;
+                ms.mptr = lp->d_don_ready;
+                ms.mbytes = (size_t)lp->don_cap * 4;
+                lp->recs.push_back(ms);
+            }
+        }
+        lp->recs.push_back(ld);
+        return BEEP_OK;
+    };
 
     // All item lists by one sort of (tier, depth, domain order) keys over the
     // flattened vertices; tier k's list is a contiguous run of the result.
@@ -2098,10 +2872,10 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         k_list_keys<<<gv, 256, 0, s>>>(lp->d_tier, d_dom, lp->d_pairs, lp->d_offs, np, N, d_keys, d_sel);
         BEEP_CUDA_TRY(cudaGetLastError());
         size_t tb = 0;
-        BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_keys, d_keys2, d_sel, d_dom, N, 0, 31, s));
+        BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_keys, d_keys2, d_sel, d_dom, N, 0, 32, s));
         BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
         BEEP_CUDA_TRY(
-            cub::DeviceRadixSort::SortPairs(ctx->scratch.ptr, tb, d_keys, d_keys2, d_sel, d_dom, N, 0, 31, s));
+            cub::DeviceRadixSort::SortPairs(ctx->scratch.ptr, tb, d_keys, d_keys2, d_sel, d_dom, N, 0, 32, s));
         k_make_items<<<std::max(1u, std::min(list_off[kTiers] / 256 + 1, 4096u)), 256, 0, s>>>(
             d_dom, list_off[kTiers], lp->d_offs, np, all_items);
         BEEP_CUDA_TRY(cudaGetLastError());
@@ -2125,7 +2899,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     uint32_t *wsc = nullptr;
     uint32_t wstride = 0;
     {
-        if (tier_depth[3 * kDepths + kWheelSlot] > 0) {
+        if (tier_depth[3 * kSlots + kWheelSlot] > 0 || tier_depth[3 * kSlots + kNbhdSlot] > 0) {
             wstride = (3 * ((tier_max[3] + 31) / 32) + 31) & ~31u;
             const size_t words = (size_t)ctx->num_sms * kLargeDfsBlocksPerSm * 8 * wstride;
             BEEP_TRY(lp->alloc(wsc, words));
@@ -2189,14 +2963,19 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         lp->recs.push_back(lr);
         if (list_cap((maxD_all + 31) / 32))
             lp->recs.push_back(lists_rec(lr));
+        if (tier_depth[3 * kSlots + kNbhdSlot] > 0)
+            lp->recs.push_back(nbdeg_rec(lr));
         uint32_t first = 0;
-        for (int d = (int)kWheelSlot; d < kDepths; ++d) {
-            const uint32_t cnt = tier_depth[3 * kDepths + d];
+        for (int sl = 0; sl < kSlots; ++sl) {
+            const uint32_t cnt = tier_depth[3 * kSlots + sl];
             if (!cnt)
                 continue;
+            const int d = sl % kDepths;
             LaunchRec ld;
-            ld.kind = d == (int)kWheelSlot ? LaunchRec::kLargeWheel : LaunchRec::kLargeDfs;
+            ld.kind = d == (int)kWheelSlot ? LaunchRec::kLargeWheel
+                                           : (d == (int)kNbhdSlot ? LaunchRec::kLargeNbhd : LaunchRec::kLargeDfs);
             ld.dend = d;
+            ld.enumerate = sl >= kDepths;
             ld.grid = ctx->num_sms * kLargeDfsBlocksPerSm;
             ld.block = 256;
             ld.bt = Batch{list + first, reinterpret_cast<const uint64_t *>(boff) + first, cstart, tstart + first,
@@ -2206,7 +2985,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             ld.sink = &st.large_dfs_ms;
             ld.wsc = wsc;
             ld.wstride = wstride;
-            lp->recs.push_back(ld);
+            BEEP_TRY(push_walk(ld));
             first += cnt;
         }
     } else if (tier_n[3] > 0) {
@@ -2226,15 +3005,16 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         BEEP_CUDA_TRY(cudaStreamSynchronize(s));
         struct R {
             uint64_t item;
-            uint32_t D, j0, dend;
+            uint32_t D, j0, dend; // dend: the depth slot
             uint64_t words; // bitmap rows [rlo, D) of D bits and their word lists
         };
         std::vector<R> rs(nl);
         for (uint32_t i = 0; i < nl; ++i) {
             const DevPlan &pl = hp[(uint32_t)(litems[i] >> 32)].pl;
             const uint32_t D = lD[i], rlo = pl.rows_needed == 2 ? 0u : (pl.rows_needed == 1 ? lj[i] : D);
-            const uint64_t words = large_root_words(D, rlo);
-            rs[i] = R{litems[i], D, lj[i], depth_slot(pl, 4), words};
+            const uint64_t words = large_root_words(D, rlo, pl.nbhd != kNbNone);
+            const PairDev &pdv = hp[(uint32_t)(litems[i] >> 32)];
+            rs[i] = R{litems[i], D, lj[i], depth_slot(pl, 4, pdv.en.out != nullptr), words};
         }
         std::sort(rs.begin(), rs.end(), [](const R &a, const R &b) { return a.D > b.D; });
         // batch boundaries and the arena size (largest batch)
@@ -2324,10 +3104,19 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             lp->recs.push_back(lr);
             if (list_cap((bmaxD + 31) / 32))
                 lp->recs.push_back(lists_rec(lr));
+            bool any_nbhd = false;
+            for (size_t i = i0; i < i1; ++i)
+                any_nbhd |= rs[i].dend == kNbhdSlot;
+            if (any_nbhd)
+                lp->recs.push_back(nbdeg_rec(lr));
             for (size_t gi = 0; gi < groups.size(); ++gi) {
                 LaunchRec ld;
-                ld.dend = (int)rs[i0 + groups[gi].first].dend;
-                ld.kind = ld.dend == (int)kWheelSlot ? LaunchRec::kLargeWheel : LaunchRec::kLargeDfs;
+                const uint32_t slot = rs[i0 + groups[gi].first].dend; // depth slot
+                ld.dend = (int)(slot % kDepths);
+                ld.enumerate = slot >= (uint32_t)kDepths;
+                ld.kind = ld.dend == (int)kWheelSlot
+                              ? LaunchRec::kLargeWheel
+                              : (ld.dend == (int)kNbhdSlot ? LaunchRec::kLargeNbhd : LaunchRec::kLargeDfs);
                 ld.grid = ctx->num_sms * kLargeDfsBlocksPerSm;
                 ld.block = 256;
                 ld.bt = Batch{d_bitem + groups[gi].first, d_boff + groups[gi].first, d_cs, d_ts + ts_off[gi],
@@ -2337,7 +3126,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
                 ld.sink = &st.large_dfs_ms;
                 ld.wsc = wsc;
                 ld.wstride = wstride;
-                lp->recs.push_back(ld);
+                BEEP_TRY(push_walk(ld));
             }
         }
     }
@@ -2353,17 +3142,19 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         // 32-bit words per row: 8 (4 x 64 bits) in the thread-mode sub-tier
         const uint32_t W = sub == 0 ? 2 * kThreadNW : (maxD + 31) / 32;
         const size_t pad = (maxD + 4) & ~3u;
-        const size_t smem = (4 * pad + (size_t)maxD * W) * 4;
+        const size_t nslots = hash_slots(maxD); // the domain hash: nslots ids and nslots 16-bit indices
+        const size_t smem = (4 * pad + nslots + nslots / 2 + (size_t)maxD * W) * 4;
         const int block = sub == 0 ? 256 : 1024;
         const int per_sm = std::max(1, (int)std::min<size_t>(2048 / block, (200 * 1024) / (smem + 1024)));
         uint32_t first = 0;
-        for (int d = 3; d < kDepths; ++d) {
-            const uint32_t cnt = tier_depth[k * kDepths + d];
+        for (int sl = 0; sl < kSlots; ++sl) {
+            const uint32_t cnt = tier_depth[k * kSlots + sl];
             if (!cnt)
                 continue;
             LaunchRec r;
             r.kind = LaunchRec::kMedium;
-            r.dend = d;
+            r.dend = sl % kDepths;
+            r.enumerate = sl >= kDepths;
             r.group = sub == 0 ? 0 : 32;
             r.grid = ctx->num_sms * per_sm;
             r.block = block;
@@ -2373,6 +3164,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             r.maxD = maxD;
             r.cursor = cursor();
             r.sink = &st.medium_ms;
+            r.tail_slot = 1;
             lp->recs.push_back(r);
             first += cnt;
         }
@@ -2382,9 +3174,9 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         uint64_t *list = nullptr;
         BEEP_TRY(make_list(0, list));
         uint32_t first = 0;
-        for (int d = 3; d < kDepths; ++d) {
-            // the list is sorted by (depth, domain): tiny domains first
-            const uint32_t n_tiny = tiny_depth[d], n_rest = tier_depth[d] - tiny_depth[d];
+        for (int sl = 0; sl < kSlots; ++sl) {
+            // the list is sorted by (depth slot, domain): tiny domains first
+            const uint32_t n_tiny = tiny_depth[sl], n_rest = tier_depth[sl] - tiny_depth[sl];
             for (int part = 0; part < 2; ++part) {
                 const uint32_t cnt = part == 0 ? n_tiny : n_rest;
                 if (!cnt)
@@ -2393,7 +3185,8 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
                 const int per_block = kSmallWarps * 32 / group;
                 LaunchRec r;
                 r.kind = LaunchRec::kSmall;
-                r.dend = d;
+                r.dend = sl % kDepths;
+                r.enumerate = sl >= kDepths;
                 r.group = group;
                 r.grid = (int)std::min<int64_t>(((int64_t)cnt + per_block - 1) / per_block,
                                                 (int64_t)ctx->num_sms * 8);
@@ -2401,6 +3194,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
                 r.items = list + first;
                 r.n = cnt;
                 r.sink = &st.small_ms;
+                r.tail_slot = 0;
                 lp->recs.push_back(r);
                 first += cnt;
             }
@@ -2426,13 +3220,14 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         BEEP_CUDA_TRY(cub::DeviceScan::InclusiveSum(ctx->scratch.ptr, tb, tasks, tstart + 1, nl, s));
         BEEP_CUDA_TRY(cudaMemsetAsync(tstart, 0, 4, s));
         uint32_t first = 0;
-        for (int d = 3; d < kDepths; ++d) {
-            const uint32_t cnt = tier_depth[4 * kDepths + d];
+        for (int sl = 0; sl < kSlots; ++sl) {
+            const uint32_t cnt = tier_depth[4 * kSlots + sl];
             if (!cnt)
                 continue;
             LaunchRec r;
             r.kind = LaunchRec::kGeneral;
-            r.dend = d;
+            r.dend = sl % kDepths;
+            r.enumerate = sl >= kDepths;
             r.grid = ctx->num_sms * 8;
             r.block = 256;
             r.items = list + first;
@@ -2449,7 +3244,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         if (r.kind == LaunchRec::kMedium) {
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
-        if (lp->enumerate)                                                                                         \
+        if (r.enumerate)                                                                                           \
             BEEP_TRY((set_medium_attr<D, true>(r.smem)));                                                          \
         else                                                                                                       \
             BEEP_TRY((set_medium_attr<D, false>(r.smem)));                                                         \
@@ -2457,6 +3252,9 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             BEEP_DEPTH_SWITCH(r.dend, BEEP_CASE)
 #undef BEEP_CASE
         }
+    lp->nexit = (uint32_t)lp->recs.size();
+    BEEP_TRY(lp->alloc(lp->d_exit, 2 * (size_t)lp->nexit));
+    BEEP_TRY(ctx->host_results(lp->host_words(), &lp->h_counts));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s)); // planning buffers are final
     tr.mark("lists");
     *out = std::move(lp);
@@ -2464,13 +3262,21 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
 }
 
 namespace {
-beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats &st,
+beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, bool stall_test, beep_stats &st,
                   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> *ev,
                   std::vector<double *> *sinks) {
     cudaStream_t s = ctx->stream;
     const uint32_t np = lp->np;
-    BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_counts, 0, (3 * (size_t)np + kAux) * 8, s));
+    BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_counts, 0, ((kPairWords + 1) * (size_t)np + kAux) * 8, s));
     BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_cursors, 0, lp->ncursors * 4, s));
+    if (lp->ndon) {
+        BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_don_ctl, 0, (size_t)lp->ndon * kDonWords * 4, s));
+        if (stall_test) // one phantom donated task that no donor publishes: every wait runs out
+            for (uint32_t i = 0; i < lp->ndon; ++i)
+                BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_don_ctl + (size_t)i * kDonWords + kDonPending, 1, 1, s));
+    }
+    if (timing && lp->nexit)
+        BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_exit, 0, 2 * (size_t)lp->nexit * 8, s));
     // The tiers are independent: large on the call's stream, medium and small
     // on two side streams forked from it and joined back at the end.
     bool have_medium = false, have_small = false;
@@ -2485,7 +3291,9 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats
         BEEP_CUDA_TRY(cudaStreamWaitEvent(ctx->side[0], ctx->ev_fork, 0));
         BEEP_CUDA_TRY(cudaStreamWaitEvent(ctx->side[1], ctx->ev_fork, 0));
     }
-    for (auto &r : lp->recs) {
+    for (size_t ri = 0; ri < lp->recs.size(); ++ri) {
+        const LaunchRec &r = lp->recs[ri];
+        unsigned long long *ex = timing ? lp->d_exit + 2 * ri : nullptr;
         cudaStream_t rs = s;
         if (fork && r.kind == LaunchRec::kMedium)
             rs = ctx->side[0];
@@ -2513,31 +3321,45 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats
             st.large_encode_launches++;
             break;
         case LaunchRec::kLargeDfs:
-            if (lp->enumerate)
+            if (r.enumerate)
                 BEEP_TRY(launch_large_dfs<true>(r.dend, r.grid, rs, lp->d_pairs, r.bt,
-                                                static_cast<const uint32_t *>(r.mptr), r.cursor));
+                                                static_cast<const uint32_t *>(r.mptr), r.cursor, r.don, ex));
             else
                 BEEP_TRY(launch_large_dfs<false>(r.dend, r.grid, rs, lp->d_pairs, r.bt,
-                                                 static_cast<const uint32_t *>(r.mptr), r.cursor));
+                                                 static_cast<const uint32_t *>(r.mptr), r.cursor, r.don, ex));
+            st.large_dfs_launches++;
+            break;
+        case LaunchRec::kLargeNbDeg:
+            k_large_nbdeg<<<r.grid, r.block, 0, rs>>>(lp->d_pairs, r.bt, static_cast<uint32_t *>(r.mptr));
+            BEEP_CUDA_TRY(cudaGetLastError());
+            st.large_encode_launches++;
+            break;
+        case LaunchRec::kLargeNbhd:
+            k_large_nbhd<<<r.grid, r.block, 0, rs>>>(lp->d_pairs, r.bt, static_cast<const uint32_t *>(r.mptr),
+                                                     r.cursor, r.wsc, r.wstride, ex);
+            BEEP_CUDA_TRY(cudaGetLastError());
             st.large_dfs_launches++;
             break;
         case LaunchRec::kLargeWheel:
             k_large_wheel<<<r.grid, r.block, 0, rs>>>(lp->d_pairs, r.bt, static_cast<const uint32_t *>(r.mptr),
-                                                      r.cursor, r.wsc, r.wstride);
+                                                      r.cursor, r.wsc, r.wstride, ex);
             BEEP_CUDA_TRY(cudaGetLastError());
             st.large_dfs_launches++;
             break;
         case LaunchRec::kMedium:
 #define BEEP_CASE(D)                                                                                               \
     case D:                                                                                                        \
-        if (lp->enumerate && r.group == 0)                                                                         \
-            k_medium<D, true, 0><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);    \
-        else if (lp->enumerate)                                                                                    \
-            k_medium<D, true, 32><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);   \
+        if (r.enumerate && r.group == 0)                                                                           \
+            k_medium<D, true, 0><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD, ex); \
+        else if (r.enumerate)                                                                                      \
+            k_medium<D, true, 32><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD,    \
+                                                                   ex);                                           \
         else if (r.group == 0)                                                                                     \
-            k_medium<D, false, 0><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);   \
+            k_medium<D, false, 0><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD,    \
+                                                                   ex);                                           \
         else                                                                                                       \
-            k_medium<D, false, 32><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD);  \
+            k_medium<D, false, 32><<<r.grid, r.block, r.smem, rs>>>(lp->d_pairs, r.items, r.n, r.cursor, r.maxD,   \
+                                                                    ex);                                          \
         break;
             BEEP_DEPTH_SWITCH(r.dend, BEEP_CASE)
 #undef BEEP_CASE
@@ -2545,17 +3367,17 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats
             st.medium_launches++;
             break;
         case LaunchRec::kGeneral:
-            if (lp->enumerate)
+            if (r.enumerate)
                 BEEP_TRY(launch_general<true>(r.dend, r.grid, rs, lp->d_pairs, r.items, r.tstart, r.n, r.cursor));
             else
                 BEEP_TRY(launch_general<false>(r.dend, r.grid, rs, lp->d_pairs, r.items, r.tstart, r.n, r.cursor));
             st.general_launches++;
             break;
         case LaunchRec::kSmall:
-            if (lp->enumerate)
-                BEEP_TRY(launch_small<true>(r.dend, r.group, r.grid, rs, lp->d_pairs, r.items, r.n));
+            if (r.enumerate)
+                BEEP_TRY(launch_small<true>(r.dend, r.group, r.grid, rs, lp->d_pairs, r.items, r.n, ex));
             else
-                BEEP_TRY(launch_small<false>(r.dend, r.group, r.grid, rs, lp->d_pairs, r.items, r.n));
+                BEEP_TRY(launch_small<false>(r.dend, r.group, r.grid, rs, lp->d_pairs, r.items, r.n, ex));
             st.small_launches++;
             break;
         }
@@ -2577,6 +3399,38 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, beep_stats
 }
 } // namespace
 
+// The read-back a run ends with: the (count, flag) words of every pair, the
+// donation control blocks and (timing) the launches' exit times.
+static cudaError_t readback(LaunchPlan *lp, cudaStream_t s, bool timing) {
+    cudaError_t e =
+        cudaMemcpyAsync(lp->h_counts, lp->d_counts, kPairWords * (size_t)lp->np * 8, cudaMemcpyDeviceToHost, s);
+    unsigned long long *tel = lp->h_counts + kPairWords * (size_t)lp->np + kAux;
+    if (e == cudaSuccess && lp->ndon)
+        e = cudaMemcpyAsync(tel, lp->d_don_ctl, (size_t)lp->ndon * kDonWords * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && timing && lp->nexit)
+        e = cudaMemcpyAsync(tel + (size_t)lp->ndon * kDonWords / 2, lp->d_exit, 2 * (size_t)lp->nexit * 8,
+                            cudaMemcpyDeviceToHost, s);
+    return e;
+}
+
+// Donation totals of the last run; BEEP_ERR_TIMEOUT when a bounded wait ran out.
+static beep_status donation_result(const LaunchPlan *lp, uint64_t *donated) {
+    const unsigned *ctl = reinterpret_cast<const unsigned *>(lp->h_counts + kPairWords * (size_t)lp->np + kAux);
+    uint64_t d = 0;
+    bool timed_out = false;
+    for (uint32_t i = 0; i < lp->ndon; ++i) {
+        d += ctl[(size_t)i * kDonWords + kDonCount];
+        timed_out |= ctl[(size_t)i * kDonWords + kDonError] != 0;
+    }
+    if (donated)
+        *donated = d;
+    if (timed_out)
+        return fail(BEEP_ERR_TIMEOUT, "a warp of the large tier waited for donated work longer than the wait "
+                                      "timeout with no progress anywhere (beep_ctx_set_wait_timeout); the counts of "
+                                      "this run are incomplete");
+    return BEEP_OK;
+}
+
 beep_status capture_plan(Ctx *ctx, LaunchPlan *lp) {
     if (lp->exec)
         return BEEP_OK;
@@ -2584,7 +3438,7 @@ beep_status capture_plan(Ctx *ctx, LaunchPlan *lp) {
     // the captured read-back needs a host buffer that no other call reuses
     if (!lp->own_h_counts) {
         unsigned long long *h = nullptr;
-        BEEP_CUDA_TRY(cudaMallocHost(&h, (2 * (size_t)lp->np + kAux) * sizeof(unsigned long long)));
+        BEEP_CUDA_TRY(cudaMallocHost(&h, lp->host_words() * sizeof(unsigned long long)));
         lp->h_counts = h;
         lp->own_h_counts = true;
     }
@@ -2592,8 +3446,8 @@ beep_status capture_plan(Ctx *ctx, LaunchPlan *lp) {
     std::memset(&scratch_st, 0, sizeof(scratch_st));
     cudaGraph_t graph = nullptr;
     BEEP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    beep_status rc = issue(ctx, lp, false, false, scratch_st, nullptr, nullptr);
-    cudaError_t ce = cudaMemcpyAsync(lp->h_counts, lp->d_counts, 2 * (size_t)lp->np * 8, cudaMemcpyDeviceToHost, s);
+    beep_status rc = issue(ctx, lp, false, false, false, scratch_st, nullptr, nullptr);
+    cudaError_t ce = readback(lp, s, false);
     cudaError_t e = cudaStreamEndCapture(s, &graph);
     if (rc != BEEP_OK) {
         if (graph)
@@ -2629,19 +3483,21 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
             st.kernel_launches += r.kind != LaunchRec::kMemset;
     } else {
         st.kernel_launches = lp->st.kernel_launches;
-        BEEP_TRY(issue(ctx, lp, timing, (options & BEEP_OPT_SERIAL_TIERS) != 0, st, &ev, &sinks));
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, 2 * (size_t)lp->np * 8, cudaMemcpyDeviceToHost, s));
+        BEEP_TRY(issue(ctx, lp, timing, (options & BEEP_OPT_SERIAL_TIERS) != 0,
+                       (options & BEEP_OPT_WAIT_STALL_TEST) != 0, st, &ev, &sinks));
+        BEEP_CUDA_TRY(readback(lp, s, timing));
     }
     if (timing)
         cudaEventRecord(e1, s);
     if (lp->np > 0 && (options & BEEP_OPT_ALG_BYTES)) {
-        unsigned long long *d_bytes = lp->d_counts + 3 * (size_t)lp->np;
+        unsigned long long *d_bytes = lp->d_counts + (kPairWords + 1) * (size_t)lp->np;
         BEEP_CUDA_TRY(cudaMemsetAsync(d_bytes, 0, kAux * 8, s));
         const int gv = std::max(1, (int)std::min<uint64_t>((lp->N + 255) / 256, (uint64_t)ctx->num_sms * 32));
         k_alg_bytes<<<gv, 256, 0, s>>>(lp->d_pairs, lp->d_offs, lp->np, lp->d_tier, lp->N, d_bytes);
         BEEP_CUDA_TRY(cudaGetLastError());
         st.kernel_launches += 1;
-        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts + 2 * (size_t)lp->np, d_bytes, kAux * 8, cudaMemcpyDeviceToHost, s));
+        BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts + kPairWords * (size_t)lp->np, d_bytes, kAux * 8,
+                                      cudaMemcpyDeviceToHost, s));
     }
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
     if (timing) {
@@ -2681,7 +3537,7 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
                        : st.count + c;
     }
     if (options & BEEP_OPT_ALG_BYTES) {
-        const unsigned long long *aux = lp->h_counts + 2 * (size_t)lp->np;
+        const unsigned long long *aux = lp->h_counts + kPairWords * (size_t)lp->np;
         st.small_bytes = aux[0];
         st.medium_bytes = aux[1];
         st.large_bytes = aux[2];
@@ -2690,25 +3546,44 @@ beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::
         st.alg_medium_bytes = aux[4];
         st.alg_large_bytes = aux[5];
     }
+    const beep_status don_rc = donation_result(lp, &st.donated_tasks);
+    if (timing && !lp->exec) {
+        // per tier, the longest spread between a launch's first and last warp
+        // exit: the time from "every item taken" to "every item done"
+        const unsigned long long *ex =
+            lp->h_counts + kPairWords * (size_t)lp->np + kAux + (size_t)lp->ndon * kDonWords / 2;
+        double *tails[3] = {&st.small_tail_ms, &st.medium_tail_ms, &st.large_tail_ms};
+        for (size_t ri = 0; ri < lp->recs.size(); ++ri) {
+            const int slot = lp->recs[ri].tail_slot;
+            if (slot < 0 || !ex[2 * ri + 1])
+                continue;
+            const unsigned long long first = ~ex[2 * ri], last = ex[2 * ri + 1];
+            *tails[slot] = std::max(*tails[slot], (double)(last - first) / 1e6);
+        }
+    }
     if (stats)
         *stats = st;
+    return don_rc;
+}
+
+beep_status launch_plan_async(Ctx *ctx, LaunchPlan *lp, unsigned long long *h_buf) {
+    // the caller's pinned buffer (plan_host_words words) receives the
+    // read-back: no pinned allocation or free on a server's latency path
+    // (cudaFreeHost waits for the whole device)
+    if (lp->h_counts && lp->own_h_counts)
+        cudaFreeHost(lp->h_counts);
+    lp->h_counts = h_buf;
+    lp->own_h_counts = false;
+    beep_stats st;
+    std::memset(&st, 0, sizeof(st));
+    BEEP_TRY(issue(ctx, lp, false, false, false, st, nullptr, nullptr));
+    BEEP_CUDA_TRY(readback(lp, ctx->stream, false));
     return BEEP_OK;
 }
 
-beep_status launch_plan_async(Ctx *ctx, LaunchPlan *lp) {
-    if (!lp->own_h_counts) {
-        unsigned long long *h = nullptr;
-        BEEP_CUDA_TRY(cudaMallocHost(&h, (2 * (size_t)lp->np + kAux) * sizeof(unsigned long long)));
-        lp->h_counts = h;
-        lp->own_h_counts = true;
-    }
-    beep_stats st;
-    std::memset(&st, 0, sizeof(st));
-    BEEP_TRY(issue(ctx, lp, false, false, st, nullptr, nullptr));
-    BEEP_CUDA_TRY(cudaMemcpyAsync(lp->h_counts, lp->d_counts, 2 * (size_t)lp->np * 8, cudaMemcpyDeviceToHost,
-                                  ctx->stream));
-    return BEEP_OK;
-}
+size_t plan_host_words(const LaunchPlan *lp) { return lp->host_words(); }
+
+beep_status plan_status(const LaunchPlan *lp) { return donation_result(lp, nullptr); }
 
 uint64_t plan_count(const LaunchPlan *lp, size_t spec_index) {
     for (uint32_t i = 0; i < lp->np; ++i)

@@ -74,6 +74,22 @@ struct DevPlan {
     uint32_t adj0;           // bit p: position p is adjacent to position 0
     uint32_t sym0;           // bit p: position p must follow position 0
     int32_t wheel4;          // the 4-wheel's plan: counted per (x1, x3) pair in closed form
+    int32_t nbhd;            // NbhdForm: in the large tier, counted from neighbourhood statistics
+};
+
+// Five-vertex central queries whose count at a root v follows from statistics
+// of the neighbourhood graph G[N(v)] (each is a cone over a 4-vertex graph H;
+// a copy counts at v when v is its earliest universal vertex, as the walk's
+// symmetry breaking counts it). d_u: degree of u in G[N(v)], E: its edges,
+// c(u, w): common neighbours of u and w in it, D = |N(v)|.
+enum NbhdForm : int32_t {
+    kNbNone = 0,
+    kNbWedgeIso = 1, // H = wedge + isolated vertex: sum_u C(d_u, 2) (D - 3)
+    kNbTwoEdges = 2, // H = two disjoint edges:     C(E, 2) - sum_u C(d_u, 2)
+    kNbTriIso = 3,   // H = triangle + isolated:    T (D - 3), T the triangles
+    kNbPath4 = 4,    // H = path on 4 vertices:     sum over edges (d_u - 1)(d_w - 1) - 3T
+    kNbPaw = 5,      // H = paw (universal vertex u after v): sum_u t_u (d_u - 2), t_u triangles at u
+    kNbDiamond = 6   // H = diamond (both universal vertices after v): sum over edges C(c(u, w), 2)
 };
 
 struct QueryPlan {
@@ -294,6 +310,9 @@ using LaunchPlanPtr = std::unique_ptr<LaunchPlan, LaunchPlanDeleter>;
 // blocks up to med_max (<= 1024), the global-arena tier above.
 struct TierCfg {
     uint32_t tiny_max = 8, small_max = 64, med_a_max = 256, med_max = 1024; // tiny_max 8: the tuner's pick on C2
+    // large tier: a walk hands half of its remaining iterations to a waiting
+    // warp when at least this many remain (0: no donation)
+    uint32_t donate_min_iters = 2;
 };
 beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t options, LaunchPlanPtr *out,
                        const TierCfg &tiers = TierCfg());
@@ -301,8 +320,13 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
 beep_status capture_plan(Ctx *ctx, LaunchPlan *lp);
 beep_status execute_plan(Ctx *ctx, LaunchPlan *lp, uint32_t options, const std::vector<PairSpec> *specs,
                          uint64_t *counts, size_t ncounts, beep_stats *stats);
-// Issue the plan and its count read-back on ctx->stream without waiting.
-beep_status launch_plan_async(Ctx *ctx, LaunchPlan *lp);
+// Issue the plan and its count read-back on ctx->stream without waiting; the
+// read-back lands in h_buf, a pinned buffer of plan_host_words(lp) words that
+// the caller owns and keeps until the stream has passed the launch.
+beep_status launch_plan_async(Ctx *ctx, LaunchPlan *lp, unsigned long long *h_buf);
+size_t plan_host_words(const LaunchPlan *lp);
+// After the stream passed the launch: BEEP_ERR_TIMEOUT if a bounded wait ran out.
+beep_status plan_status(const LaunchPlan *lp);
 // After the stream passed the launch: the count of the spec_index-th pair.
 uint64_t plan_count(const LaunchPlan *lp, size_t spec_index);
 // Kernel launches of planning plus one execution.

@@ -306,6 +306,57 @@ beep_status compile_plan(int32_t qn, const std::vector<int32_t> &rp, const std::
         }
     }
     P.wheel4 = D.wheel4;
+    // Neighbourhood statistics: a five-vertex central query at full depth is
+    // a cone over H = positions 1-4. The forms below are those whose count at
+    // a root is a sum of per-vertex and per-edge terms of G[N(root)]; the
+    // other universal vertices of H (paw: its degree-3 vertex; diamond: its
+    // two) must follow the root as the chain demands, so that the count at a
+    // root is the walk's count at that root and the tiers can be mixed.
+    D.nbhd = kNbNone;
+    if (qn == 5 && D.dend == 5 && P.central && !D.wheel4) {
+        uint32_t adj[5] = {0, 0, 0, 0, 0};
+        int edges = 0;
+        for (int p = 2; p <= 4; ++p)
+            for (int q = 1; q < p; ++q)
+                if (D.back[p] >> q & 1u) {
+                    adj[p] |= 1u << q;
+                    adj[q] |= 1u << p;
+                    ++edges;
+                }
+        int deg[4], hub = -1, hubs = 0;
+        for (int p = 1; p <= 4; ++p) {
+            deg[p - 1] = __builtin_popcount(adj[p]);
+            if (deg[p - 1] == 3) {
+                ++hubs;
+                if (hub < 0)
+                    hub = p;
+            }
+        }
+        std::sort(deg, deg + 4);
+        auto seq = [&](int a, int b, int c, int d) { return deg[0] == a && deg[1] == b && deg[2] == c && deg[3] == d; };
+        // position p must follow the root: position 1 through the split,
+        // later ones through the chain from position 1
+        auto after_root = [&](int p) { return D.pos1_after_root && (p == 1 || (after[p] >> 1 & 1u)); };
+        bool universal_after = true;
+        for (int p = 1; p <= 4; ++p)
+            if (__builtin_popcount(adj[p]) == 3)
+                universal_after = universal_after && after_root(p);
+        if (edges == 2 && seq(0, 1, 1, 2) && !D.pos1_after_root)
+            D.nbhd = kNbWedgeIso;
+        else if (edges == 2 && seq(1, 1, 1, 1) && !D.pos1_after_root)
+            D.nbhd = kNbTwoEdges;
+        else if (edges == 3 && seq(0, 2, 2, 2) && !D.pos1_after_root)
+            D.nbhd = kNbTriIso;
+        else if (edges == 3 && seq(1, 1, 2, 2) && !D.pos1_after_root)
+            D.nbhd = kNbPath4;
+        else if (edges == 4 && seq(1, 2, 2, 3) && hubs == 1 && universal_after)
+            D.nbhd = kNbPaw;
+        else if (edges == 5 && seq(2, 2, 3, 3) && hubs == 2 && universal_after)
+            D.nbhd = kNbDiamond;
+    }
+    if (D.nbhd)
+        D.rows_needed = 2; // the statistics read every row of the neighbourhood
+    P.nbhd = D.nbhd;
     out->info = P;
     out->dev = D;
     return BEEP_OK;

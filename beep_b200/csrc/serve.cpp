@@ -40,6 +40,33 @@ struct Request {
     bool finished = false;
 };
 
+// Grow-only pinned host buffer. Pinned allocation and release are slow and
+// cudaFreeHost waits for the whole device, so a slot keeps its buffers from
+// batch to batch and replaces them only to grow.
+template <typename T> struct PinnedBuf {
+    T *ptr = nullptr;
+    size_t n = 0;
+    cudaError_t reserve(size_t want) {
+        if (want <= n)
+            return cudaSuccess;
+        if (ptr)
+            cudaFreeHost(ptr);
+        ptr = nullptr;
+        n = 0;
+        const size_t grow = std::max(want, (size_t)4096);
+        cudaError_t e = cudaMallocHost(&ptr, grow * sizeof(T));
+        if (e == cudaSuccess)
+            n = grow;
+        return e;
+    }
+    void release() {
+        if (ptr)
+            cudaFreeHost(ptr);
+        ptr = nullptr;
+        n = 0;
+    }
+};
+
 struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
@@ -50,9 +77,12 @@ struct Slot {
     LaunchPlanPtr plan;
     std::vector<std::shared_ptr<Request>> reqs;
     std::vector<EnumRequest> enums;
-    std::vector<void *> dbufs;    // device tuple buffers (pool)
-    std::vector<int32_t *> hbufs; // pinned staging of the tuples
+    std::vector<void *> dbufs;     // device tuple buffers (pool)
+    std::vector<size_t> hoff;      // each request's tuples in the staging buffer
+    PinnedBuf<int32_t> tuples;     // pinned staging of the batch's tuples
+    PinnedBuf<unsigned long long> counts; // pinned read-back of the batch's counts
     std::vector<PairSpec> specs;
+    uint64_t reserved = 0;         // admission estimate of the batch in flight
 };
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
@@ -65,9 +95,14 @@ struct Server {
     beep_ctx *uctx = nullptr;
     Ctx ctx; // planning resources; its stream is switched to the slot being planned
     std::vector<Graph *> graphs;
+    std::vector<uint64_t> graph_large_bytes; // per graph: dense bitmaps of every root of degree > 1024
     std::vector<Slot> slots;
     uint32_t max_batch = 64;
     uint64_t reserve = 1ull << 30;
+    uint64_t budget = 0;      // device bytes the admission may hand out: free HBM at creation - reserve
+    uint64_t inflight = 0;    // estimates of the batches in flight
+    uint64_t max_inflight = 0;
+    uint64_t refused = 0;
     uint32_t count_options = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -86,14 +121,27 @@ struct Server {
     void loop();
     void launch(Slot &sl, std::vector<std::shared_ptr<Request>> &batch);
     void finish(Slot &sl, beep_status st, const std::string &err);
+    // Device bytes a request can take while its batch runs: its tuple buffer,
+    // the planning arrays over its graph's vertices and entries, and the
+    // large tier's bitmap arena -- at most the dense bitmaps of all the
+    // graph's roots of degree above 1024, and never more than the arena cap
+    // that planning applies (min(48 GiB, half the free memory)).
     uint64_t estimate(const Request &r) const {
         const Graph *g = graphs[r.graph];
-        return (uint64_t)r.k * (uint64_t)r.plan.info.K * 4ull + (uint64_t)g->n * 64ull + (uint64_t)g->m * 4ull;
+        const uint64_t arena = std::min<uint64_t>(graph_large_bytes[r.graph], std::min<uint64_t>(48ull << 30, budget / 2));
+        return (uint64_t)r.k * (uint64_t)r.plan.info.K * 4ull + (uint64_t)g->n * 64ull + (uint64_t)g->m * 4ull +
+               arena;
     }
 };
 
-void Server::finish(Slot &sl, beep_status st, const std::string &err) {
+void Server::finish(Slot &sl, beep_status st, const std::string &err_in) {
     const auto now = Clock::now();
+    std::string err = err_in;
+    if (st == BEEP_OK && sl.plan && (st = plan_status(sl.plan.get())) != BEEP_OK) {
+        char buf[512];
+        beep_last_error(buf, sizeof(buf));
+        err = buf;
+    }
     for (size_t i = 0; i < sl.reqs.size(); ++i) {
         Request &r = *sl.reqs[i];
         r.done = now;
@@ -107,7 +155,8 @@ void Server::finish(Slot &sl, beep_status st, const std::string &err) {
                 r.error = "the count is at least BEEP_COUNT_LIMIT (2^64 - 2^52)";
             } else if (r.k > 0) {
                 r.n_tuples = std::min<uint64_t>(r.k, r.count);
-                r.tuples.assign(sl.hbufs[i], sl.hbufs[i] + r.n_tuples * (uint64_t)r.plan.info.K);
+                const int32_t *h = sl.tuples.ptr + sl.hoff[i];
+                r.tuples.assign(h, h + r.n_tuples * (uint64_t)r.plan.info.K);
             }
             if (r.status == BEEP_OK)
                 matches += r.count;
@@ -119,11 +168,10 @@ void Server::finish(Slot &sl, beep_status st, const std::string &err) {
     for (void *p : sl.dbufs)
         if (p)
             cudaFreeAsync(p, sl.stream);
-    for (int32_t *h : sl.hbufs)
-        if (h)
-            cudaFreeHost(h);
     sl.dbufs.clear();
-    sl.hbufs.clear();
+    sl.hoff.clear();
+    inflight -= sl.reserved;
+    sl.reserved = 0;
     sl.enums.clear();
     sl.specs.clear();
     sl.reqs.clear();
@@ -142,11 +190,24 @@ void Server::launch(Slot &sl, std::vector<std::shared_ptr<Request>> &batch) {
     sl.reqs = batch;
     sl.enums.assign(batch.size(), EnumRequest{});
     sl.dbufs.assign(batch.size(), nullptr);
-    sl.hbufs.assign(batch.size(), nullptr);
+    sl.hoff.assign(batch.size(), 0);
     sl.specs.clear();
     beep_status st = BEEP_OK;
     std::string err;
     const auto start = Clock::now();
+    // tuple staging: one pinned region per slot, each request at its offset
+    size_t tuple_words = 0;
+    for (size_t i = 0; i < batch.size(); ++i) {
+        sl.hoff[i] = tuple_words;
+        tuple_words += (size_t)batch[i]->k * (size_t)batch[i]->plan.info.K;
+    }
+    if (tuple_words) {
+        cudaError_t e = sl.tuples.reserve(tuple_words);
+        if (e != cudaSuccess) {
+            st = BEEP_ERR_OUT_OF_MEMORY;
+            err = std::string("tuple staging: ") + cudaGetErrorString(e);
+        }
+    }
     for (size_t i = 0; i < batch.size() && st == BEEP_OK; ++i) {
         Request &r = *batch[i];
         r.start = start;
@@ -156,8 +217,6 @@ void Server::launch(Slot &sl, std::vector<std::shared_ptr<Request>> &batch) {
         if (r.k > 0) {
             const size_t bytes = (size_t)r.k * (size_t)r.plan.info.K * 4;
             cudaError_t e = cudaMallocFromPoolAsync(&sl.dbufs[i], bytes, ctx.pool, sl.stream);
-            if (e == cudaSuccess)
-                e = cudaMallocHost(&sl.hbufs[i], bytes);
             if (e != cudaSuccess) {
                 st = BEEP_ERR_OUT_OF_MEMORY;
                 err = std::string("tuple buffers: ") + cudaGetErrorString(e);
@@ -168,17 +227,27 @@ void Server::launch(Slot &sl, std::vector<std::shared_ptr<Request>> &batch) {
         }
         sl.specs.push_back(ps);
     }
-    for (size_t i = 0; i < sl.specs.size(); ++i)
-        if (batch[i]->k > 0)
-            sl.specs[i].en = &sl.enums[i];
+    // spec i counts request i (closed forms allowed); a first-k request also
+    // gets an enumerating spec after them, whose walk stops at k tuples
+    const size_t ncount = sl.specs.size();
+    for (size_t i = 0; i < ncount; ++i)
+        if (batch[i]->k > 0) {
+            PairSpec es = sl.specs[i];
+            es.en = &sl.enums[i];
+            sl.specs.push_back(es);
+        }
     if (st == BEEP_OK)
         st = plan_pairs(&ctx, sl.specs, count_options, &sl.plan);
+    if (st == BEEP_OK && sl.counts.reserve(plan_host_words(sl.plan.get())) != cudaSuccess) {
+        st = BEEP_ERR_OUT_OF_MEMORY;
+        err = "pinned read-back buffer";
+    }
     if (st == BEEP_OK)
-        st = launch_plan_async(&ctx, sl.plan.get());
+        st = launch_plan_async(&ctx, sl.plan.get(), sl.counts.ptr);
     if (st == BEEP_OK) {
         for (size_t i = 0; i < batch.size(); ++i)
             if (batch[i]->k > 0) {
-                cudaError_t e = cudaMemcpyAsync(sl.hbufs[i], sl.dbufs[i],
+                cudaError_t e = cudaMemcpyAsync(sl.tuples.ptr + sl.hoff[i], sl.dbufs[i],
                                                 (size_t)batch[i]->k * (size_t)batch[i]->plan.info.K * 4,
                                                 cudaMemcpyDeviceToHost, sl.stream);
                 if (e != cudaSuccess) {
@@ -225,32 +294,43 @@ void Server::loop() {
         }
         if (progressed)
             cv_done.notify_all();
-        // new batches: a free stream, pending requests and the memory to run them
+        // new batches: a free stream, pending requests and the memory to run
+        // them. A request whose estimate exceeds the whole budget can never
+        // run and is refused; one that does not fit beside the batches in
+        // flight waits for them (back-pressure), and so do the requests
+        // behind it (arrival order is kept).
         for (auto &sl : slots) {
             if (sl.busy || pending.empty())
                 continue;
-            size_t free_b = 0, total_b = 0;
-            cudaMemGetInfo(&free_b, &total_b);
-            const uint64_t budget = free_b > reserve ? free_b - reserve : 0;
             std::vector<std::shared_ptr<Request>> batch;
             uint64_t need = 0;
             while (!pending.empty() && batch.size() < max_batch) {
-                const uint64_t e = estimate(*pending.front());
-                if (!batch.empty() && need + e > budget)
-                    break;
-                if (batch.empty() && e > budget) {
-                    bool others_running = false;
-                    for (auto &o : slots)
-                        others_running |= o.busy;
-                    if (others_running)
-                        break; // wait for memory to come back
+                std::shared_ptr<Request> r = pending.front();
+                const uint64_t e = estimate(*r);
+                if (e > budget) {
+                    pending.pop_front();
+                    r->status = BEEP_ERR_OUT_OF_MEMORY;
+                    r->error = "request needs an estimated " + std::to_string(e) + " device bytes, more than the " +
+                               std::to_string(budget) + " the server may use (free HBM at creation minus the reserve)";
+                    r->start = r->done = Clock::now();
+                    r->finished = true;
+                    ++refused;
+                    progressed = true;
+                    continue;
                 }
+                if (inflight + need + e > budget)
+                    break;
                 need += e;
-                batch.push_back(pending.front());
+                batch.push_back(r);
                 pending.pop_front();
             }
+            if (progressed)
+                cv_done.notify_all();
             if (batch.empty())
                 continue;
+            sl.reserved = need;
+            inflight += need;
+            max_inflight = std::max(max_inflight, inflight);
             lk.unlock();
             launch(sl, batch);
             lk.lock();
@@ -326,6 +406,15 @@ beep_status beep_serve_create(beep_ctx *ctx, const beep_serve_options *opt, beep
         return fail(BEEP_ERR_CUDA, std::string("server setup: ") + cudaGetErrorString(e));
     }
     S.ctx.stream = S.slots[0].stream;
+    {
+        size_t free_b = 0, total_b = 0;
+        e = cudaMemGetInfo(&free_b, &total_b);
+        if (e != cudaSuccess) {
+            beep_serve_destroy(s);
+            return fail(BEEP_ERR_CUDA, std::string("server setup: ") + cudaGetErrorString(e));
+        }
+        S.budget = free_b > S.reserve ? free_b - S.reserve : 0;
+    }
     S.thr = std::thread([&S] { S.loop(); });
     *out = s;
     return BEEP_OK;
@@ -336,8 +425,20 @@ beep_status beep_serve_add_graph(beep_server *s, beep_graph *g, int32_t *graph_i
         return fail(BEEP_ERR_INVALID_ARG, "beep_serve_add_graph: bad arguments");
     if (g->impl.device != s->impl.ctx.device)
         return fail(BEEP_ERR_INVALID_ARG, "graph lives on another device");
+    // the large tier's bitmap bound of this graph: rows of ceil(D / 32) words
+    // for every root of degree D > 1024, plus their non-zero-word lists
+    std::vector<uint32_t> rp((size_t)g->impl.n + 1);
+    BEEP_CUDA_TRY(cudaSetDevice(g->impl.device));
+    BEEP_CUDA_TRY(cudaMemcpy(rp.data(), g->impl.row_ptr.ptr, rp.size() * 4, cudaMemcpyDeviceToHost));
+    uint64_t large = 0;
+    for (size_t v = 0; v + 1 < rp.size(); ++v) {
+        const uint64_t d = rp[v + 1] - rp[v];
+        if (d > 1024)
+            large += d * ((d + 31) / 32) * 4 + d * ((d + 31) / 32) / 2;
+    }
     std::lock_guard<std::mutex> lk(s->impl.mu);
     s->impl.graphs.push_back(&g->impl);
+    s->impl.graph_large_bytes.push_back(large);
     *graph_id = (int32_t)(s->impl.graphs.size() - 1);
     return BEEP_OK;
 }
@@ -422,6 +523,9 @@ beep_status beep_serve_stats_get(beep_server *s, beep_serve_stats *out) {
     out->matches = S.matches;
     out->kernel_launches = S.launches;
     out->max_batch = S.max_batch_seen;
+    out->refused = S.refused;
+    out->max_inflight_bytes = S.max_inflight;
+    out->budget_bytes = S.budget;
     if (!S.lat_ms.empty()) {
         std::vector<double> v = S.lat_ms;
         std::sort(v.begin(), v.end());
@@ -455,6 +559,8 @@ beep_status beep_serve_destroy(beep_server *s) {
         if (sl.stream)
             cudaStreamSynchronize(sl.stream);
         sl.plan.reset();
+        sl.tuples.release();
+        sl.counts.release();
         if (sl.done)
             cudaEventDestroy(sl.done);
     }

@@ -111,6 +111,11 @@ def profiled_traffic() -> dict:
     return out
 
 
+def note(msg: str) -> None:
+    """Progress on stderr (the JSON line stays alone on stdout)."""
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def gen_graph(kind, args):
     import beep_b200 as B
 
@@ -384,7 +389,8 @@ def reference_arm(args, wl):
 # ---------------------------------------------------------------------------
 # plain workloads (our arm)
 # ---------------------------------------------------------------------------
-def plain_workload(args, wl, world, rank, local, steps, warmup, with_serial=True, with_cpu=True) -> dict:
+def plain_workload(args, wl, world, rank, local, steps, warmup, with_serial=True, with_cpu=True,
+                   with_e2e=True) -> dict:
     """One plain workload timed as the module docstring describes. Returns
     the fields of its JSON object."""
     import torch
@@ -394,6 +400,7 @@ def plain_workload(args, wl, world, rank, local, steps, warmup, with_serial=True
 
     rp, col = gen_graph(*wl["graph"])
     n, m = len(rp) - 1, len(col)
+    note(f"{wl['desc']}: n={n} m={m}")
     mode = B.SGC if wl["mode"] == "sgc" else B.SGM
     stream = torch.cuda.Stream()
     ctx = B.Context(local, cuda_stream=stream.cuda_stream)
@@ -471,9 +478,11 @@ def plain_workload(args, wl, world, rank, local, steps, warmup, with_serial=True
     per_step = total // steps
     value = per_step / (ms_step / 1e3)
 
-    e_total, e_ms, _, _, _ = timed(True, steps)
-    e_ms = max_over_ranks(e_ms, world)
-    e2e_value = (e_total // steps) / (e_ms / steps / 1e3)
+    e_total, e_ms = 0, 0.0
+    if with_e2e:
+        e_total, e_ms, _, _, _ = timed(True, steps)
+        e_ms = max_over_ranks(e_ms, world)
+    e2e_value = (e_total // steps) / (e_ms / steps / 1e3) if with_e2e else None
 
     # host->device copy of one step's inputs alone (pinned buffers, same stream), to explain e2e - value
     with torch.cuda.stream(stream):
@@ -491,7 +500,8 @@ def plain_workload(args, wl, world, rank, local, steps, warmup, with_serial=True
            "config": workload_config(wl, n, m), "counts": dict(zip(wl["patterns"], counts)),
            "matches_per_step": per_step,
            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * (n + 1) + 4 * m),
-                   "d2h_bytes_per_step": 16 * len(queries), "ms_per_step": e_ms / steps, "h2d_copy_ms": h2d_ms},
+                   "d2h_bytes_per_step": 16 * len(queries), "ms_per_step": e_ms / steps if with_e2e else None,
+                   "h2d_copy_ms": h2d_ms},
            "gpu_launches": int(launches), "clocks": clocks,
            "step": "device CSR build + per-pattern peel/relabel + count" +
                    (f", roots sharded over {world} ranks (beep_count_shard) + one NCCL all-reduce of the counts"
@@ -594,6 +604,7 @@ def bench_batched(args) -> dict:
     host = [B.gen_chung_lu(*sp) for sp in specs]
     gen_s = time.perf_counter() - t0
     graphs = [B.Graph.from_csr(ctx, rp, col) for rp, col in host]
+    note(f"c4: {len(graphs)} graphs generated in {gen_s:.1f} s, {sum(len(c) for _, c in host)} directed edges")
     pats = [B.Query.from_edges(q) for q in P.central_patterns(4) + P.central_patterns(5)]
     pairs = [(gi, qi) for gi in range(len(graphs)) for qi in range(len(pats))]
 
@@ -610,10 +621,12 @@ def bench_batched(args) -> dict:
     for gi, qi in pairs:
         plain(gi, qi)
     first_pass_s = time.perf_counter() - t0
+    note(f"c4: first pass of the per-pair loop {first_pass_s:.1f} s")
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     plain_counts = [plain(gi, qi) for gi, qi in pairs]
     plain_s = time.perf_counter() - t0
+    note(f"c4: per-pair loop {plain_s:.1f} s")
     batch = B.Batch(ctx)
     for gi, qi in pairs:
         batch.add(graphs[gi], pats[qi])
@@ -625,6 +638,7 @@ def bench_batched(args) -> dict:
     t0 = time.perf_counter()
     first = batch.run()  # plans and captures
     plan_s = time.perf_counter() - t0
+    note(f"c4: plan + capture + first replay {plan_s:.1f} s")
     clocks = ClockSampler(0)
     clocks.start()
     for _ in range(args.warmup):
@@ -687,6 +701,7 @@ def bench_served(args) -> dict:
         rp, col = B.gen_chung_lu(n, 16.0, 2.1, 17000 + i)
         host.append((rp, col))
         graphs.append(B.Graph.from_csr(ctx, rp, col))
+    note(f"c5: {len(graphs)} graphs, {sum(len(c) for _, c in host)} directed edges")
     names = ["triangle", "diamond", "k4", "tailed_triangle", "w5", "k5"]
     queries = {nm: B.Query.from_edges(P.NAMED[nm]) for nm in names}
     n_req = int(args.c5_rate * args.c5_seconds)
@@ -708,6 +723,7 @@ def bench_served(args) -> dict:
         else:
             serial.append(B.count(graphs[gi], queries[nm]))
     serial_s = time.perf_counter() - t0
+    note(f"c5: serial run of {n_req} requests {serial_s:.1f} s")
     srv = B.Server(ctx, max_batch=args.c5_max_batch, streams=args.c5_streams)
     gids = [srv.add_graph(g) for g in graphs]
     start = time.perf_counter()
@@ -814,7 +830,7 @@ def main():
                     k_steps = args.steps if key == "c1" else args.c3_steps
                     k_warm = args.warmup if key == "c1" else 0
                     r = plain_workload(args, WORKLOADS[key], 1, 0, 0, k_steps, k_warm, with_serial=(key == "c1"),
-                                       with_cpu=(key == "c1"))
+                                       with_cpu=(key == "c1"), with_e2e=(key == "c1"))
                 elif key == "c4":
                     r = bench_batched(argparse.Namespace(**{**vars(args), "steps": args.c4_steps,
                                                             "warmup": min(args.warmup, 2)}))

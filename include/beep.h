@@ -81,8 +81,12 @@ const char *beep_status_string(beep_status s);
  * (subgraph_matching.cuh:113, :180). */
 beep_status beep_ctx_create(int device, void *cuda_stream, beep_ctx **out);
 beep_status beep_ctx_destroy(beep_ctx *ctx);
-/* Bound (milliseconds) on every device-side wait of the context's kernels;
- * a wait that runs out ends its kernel with BEEP_ERR_TIMEOUT. */
+/* Bound (milliseconds, default 1000) on every device-side wait of the
+ * context's kernels: the large tier's warps that wait for donated work give
+ * up after this long without progress anywhere on the GPU (no donation, no
+ * finished task, no heartbeat of a running walk); the call then returns
+ * BEEP_ERR_TIMEOUT and the context stays usable. Applies to calls planned
+ * after it is set. */
 beep_status beep_ctx_set_wait_timeout(beep_ctx *ctx, double ms);
 /* Number of the library's own kernels launched on this context so far. */
 beep_status beep_ctx_kernel_launches(const beep_ctx *ctx, uint64_t *out);
@@ -152,6 +156,11 @@ typedef struct beep_plan_info {
                               last position) */
     int32_t wheel4;        /* 1: the 4-wheel's plan (positions 1-4 a 4-cycle around the
                               root); counts are summed once per (x1, x3) pair in closed form */
+    int32_t nbhd;          /* > 0: a five-vertex query counted at the large tier's roots from
+                              statistics of the root's neighbourhood graph (degrees, edges,
+                              common neighbours per edge); 1 wedge + isolated vertex, 2 two
+                              disjoint edges, 3 triangle + isolated vertex, 4 path, 5 paw,
+                              6 diamond (the query minus its root) */
 } beep_plan_info;
 beep_status beep_query_plan(const beep_query *q, beep_mode mode, beep_plan_info *out);
 
@@ -170,7 +179,15 @@ enum {
     /* Launch the kernel tiers one after another on the call's stream instead
      * of overlapping them on side streams (with BEEP_OPT_TIMING: per-kernel
      * times that are each kernel's own). */
-    BEEP_OPT_SERIAL_TIERS = 1u << 5
+    BEEP_OPT_SERIAL_TIERS = 1u << 5,
+    /* Test of the bounded device waits: the large tier's walk launches start
+     * with one donated task that no donor ever publishes, so every warp that
+     * waits for donated work runs out its wait (beep_ctx_set_wait_timeout)
+     * and the call returns BEEP_ERR_TIMEOUT. No effect without large roots. */
+    BEEP_OPT_WAIT_STALL_TEST = 1u << 6,
+    /* Count the large tier's roots of every query by walking, even where the
+     * plan has a neighbourhood-statistics form (beep_plan_info.nbhd). */
+    BEEP_OPT_NO_NBHD = 1u << 7
 };
 
 typedef struct beep_stats {
@@ -202,6 +219,11 @@ typedef struct beep_stats {
      * adjacency traffic of building each root's neighbourhood bitmap from the
      * CSR, whatever the kernels actually read */
     uint64_t alg_small_bytes, alg_medium_bytes, alg_large_bytes;
+    /* BEEP_OPT_TIMING: per tier, the longest time of a launch from its first
+     * to its last warp's exit -- from "every item taken" to "every item done",
+     * the load-imbalance tail */
+    double small_tail_ms, medium_tail_ms, large_tail_ms;
+    uint64_t donated_tasks;     /* subtrees the large tier's walks handed to waiting warps */
 } beep_stats;
 
 /* Count matches. Replaces SG_Match::run + count_subgraphs + final_counter
@@ -244,12 +266,17 @@ enum {
     BEEP_OPT_NO_GRAPH = 1u << 4
 };
 /* Domain-size limits of the kernel tiers a batch plans with (each clamped to
- * its kernel's bound: 16, 64, 256, 1024; defaults 8, 64, 256, 1024). A root whose search domain has D
- * vertices goes to 8-lane groups if D <= tiny_max, warp groups if
- * D <= small_max, thread-walker blocks if D <= med_a_max, warp-walker blocks if
- * D <= med_max, and the global-arena tier above. */
+ * its kernel's bound: 16, 64, 256, 1024; defaults 8, 64, 256, 1024), and the
+ * large tier's donation threshold. A root whose search domain has D vertices
+ * goes to 8-lane groups if D <= tiny_max, warp groups if D <= small_max,
+ * thread-walker blocks if D <= med_a_max, warp-walker blocks if D <= med_max,
+ * and the global-arena tier above. In the global-arena tier a warp walking a
+ * level hands the upper half of its remaining iterations (32 bitmap words
+ * each) to a waiting warp when at least donate_min_iters remain (default 2;
+ * 0 turns donation off). */
 typedef struct beep_tier_cfg {
     uint32_t tiny_max, small_max, med_a_max, med_max;
+    uint32_t donate_min_iters;
 } beep_tier_cfg;
 beep_status beep_batch_create(beep_ctx *ctx, beep_batch **out);
 beep_status beep_batch_add(beep_batch *b, beep_graph *g, const beep_query *q, beep_mode mode, uint32_t *index);
@@ -259,11 +286,11 @@ beep_status beep_batch_run(beep_batch *b, uint32_t options, uint64_t *counts, be
 beep_status beep_batch_size(const beep_batch *b, uint32_t *out);
 beep_status beep_batch_destroy(beep_batch *b);
 /* Pick the batch's tier limits by measurement: coordinate descent over
- * tiny_max {0, 8, 16}, small_max {32, 64}, med_a_max {128, 256} and
- * med_max {512, 1024}, each candidate planned and run once (no CUDA graph)
- * with its counting kernels timed by CUDA events; later runs plan with the
- * fastest. Counts do not depend on the limits. chosen and best_count_ms may be
- * NULL. */
+ * tiny_max {0, 8, 16}, small_max {32, 64}, med_a_max {128, 256}, med_max
+ * {512, 1024} and donate_min_iters {2, 4, 16}, each candidate planned and run
+ * once (no CUDA graph) with its counting kernels timed by CUDA events; later
+ * runs plan with the fastest. Counts do not depend on the choice. chosen and
+ * best_count_ms may be NULL. */
 beep_status beep_batch_autotune(beep_batch *b, uint32_t options, beep_tier_cfg *chosen, double *best_count_ms);
 beep_status beep_batch_set_tiers(beep_batch *b, const beep_tier_cfg *cfg);
 
@@ -271,7 +298,12 @@ beep_status beep_batch_set_tiers(beep_batch *b, const beep_tier_cfg *cfg);
 
 /* A request server over resident graphs with continuous batching. Requests
  * are queued by beep_serve_submit and return at once; a scheduler thread
- * admits them while the free HBM stays above a reserve, plans whatever has
+ * admits them in arrival order while the estimates of the batches in flight
+ * fit the budget (free HBM at creation minus the reserve; the estimate covers
+ * a request's tuple buffer, planning arrays and the large tier's bitmap
+ * arena): a request that does not fit waits for running batches to finish,
+ * and one that exceeds the whole budget is refused with
+ * BEEP_ERR_OUT_OF_MEMORY instead of running out of memory. It plans whatever has
  * arrived as one multi-pair call and launches it on one of several streams
  * without waiting, so batches overlap on the device and requests arriving
  * meanwhile join the next batch as soon as a stream frees up. The reference
@@ -299,6 +331,9 @@ typedef struct beep_serve_stats {
     double p50_ms, p99_ms, mean_ms, max_ms;
     double span_s;              /* first arrival to last completion */
     double max_batch;
+    uint64_t refused;           /* requests whose estimate exceeds the budget (BEEP_ERR_OUT_OF_MEMORY) */
+    uint64_t max_inflight_bytes;/* largest sum of estimates of the batches in flight at once */
+    uint64_t budget_bytes;      /* device bytes admission may hand out: free HBM at creation - reserve */
 } beep_serve_stats;
 beep_status beep_serve_create(beep_ctx *ctx, const beep_serve_options *opt, beep_server **out);
 beep_status beep_serve_add_graph(beep_server *s, beep_graph *g, int32_t *graph_id);

@@ -1,0 +1,86 @@
+"""Neighbourhood statistics of the large tier: six five-vertex central
+queries whose count at a root follows from degrees, edges and per-edge common
+neighbours of the root's neighbourhood graph. Their counts must equal the
+oracle's (bit-exact) and the walk's (the same call with BEEP_OPT_NO_NBHD),
+under every labelling of the query."""
+import random
+
+import numpy as np
+import pytest
+
+import beep_b200 as B
+from beep_b200 import patterns as P
+from oracle import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+
+FORMS = {6: 1, 7: 2, 9: 3, 10: 4, 11: 5, 13: 6}  # central pattern index -> beep_plan_info.nbhd
+
+
+def csr_from_pairs(n, pairs):
+    adj = [set() for _ in range(n)]
+    for a, b in pairs:
+        if a != b:
+            adj[a].add(b)
+            adj[b].add(a)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum([len(x) for x in adj])
+    col = np.array([w for x in adj for w in sorted(x)], np.int32)
+    return rp, col
+
+
+def hubs(n_leaves, p, seed, n_hubs=2):
+    """n_hubs hubs over n_leaves leaves with G(n_leaves, p) among the leaves:
+    the hubs are large roots (degree > 1024), the rest small."""
+    rng = np.random.default_rng(seed)
+    pairs = [(h, n_hubs + i) for h in range(n_hubs) for i in range(n_leaves)]
+    m = int(p * n_leaves * (n_leaves - 1) / 2)
+    a = rng.integers(n_hubs, n_hubs + n_leaves, size=m)
+    b = rng.integers(n_hubs, n_hubs + n_leaves, size=m)
+    pairs += list(zip(a.tolist(), b.tolist()))
+    return csr_from_pairs(n_hubs + n_leaves, pairs)
+
+
+def relabel(q, seed):
+    perm = list(range(5))
+    random.Random(seed).shuffle(perm)
+    return sorted({(perm[a], perm[b]) for a, b in q})
+
+
+def test_forms_are_detected():
+    pats = P.central_patterns(4) + P.central_patterns(5)
+    for i, q in enumerate(pats):
+        for seed in range(4):
+            assert B.Query.from_edges(relabel(q, seed) if len(q) >= 8 and i >= 4 else q).plan()["nbhd"] == \
+                FORMS.get(i, 0), i
+
+
+def test_forms_match_oracle(ctx):
+    rp, col = hubs(1400, 0.012, 3)
+    g = B.Graph.from_csr(ctx, rp, col)
+    pats = P.central_patterns(4) + P.central_patterns(5)
+    for i in FORMS:
+        for seed in (0, 1):
+            q = relabel(pats[i], seed)
+            exp = O.count(rp, col, q, apply_root_cap=False)["count"]
+            c, st = B.count(g, q, B.SGM, B.OPT_TIMING, stats=True)
+            assert c == exp, (i, seed)
+            assert st["roots_large"] >= 1, (i, st["roots_large"])
+            assert B.count(g, q, B.SGM, B.OPT_NO_NBHD) == exp, (i, seed)
+    g.close()
+
+
+def test_forms_with_word_lists_match_the_walk(ctx):
+    """Hubs of degree 9,000: rows of 282 words carry non-zero-word lists."""
+    rp, col = hubs(9000, 0.0012, 5, n_hubs=3)
+    g = B.Graph.from_csr(ctx, rp, col)
+    pats = P.central_patterns(4) + P.central_patterns(5)
+    b = B.Batch(ctx)
+    for i in FORMS:
+        b.add(g, pats[i])
+    got = b.run()
+    walk = b.run(B.OPT_NO_NBHD | B.OPT_NO_GRAPH)
+    assert got == walk
+    assert all(c > 0 for c in got)
+    b.close()
+    g.close()

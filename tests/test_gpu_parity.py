@@ -334,11 +334,15 @@ def test_root_shards_sum_and_match_oracle(ctx):
     g.close()
 
 
-def test_c3_k5_sampled_roots(ctx):
+def test_c3_sampled_roots(ctx):
     """Full-size R-MAT s22 ef28 (seed 11): the 5-clique count of 1 root in
     997 (by input id) against the oracle's independent clique counter on the
-    same roots, and the sum of sgm shards against the full count for a
-    sample of shards."""
+    same roots, and the 4-wheel count of another shard of 1,701 roots (degrees
+    up to 5,140, 31 of them in the large tier) against the oracle's count of
+    those roots, recorded in tests/golden/c3_samples.json by
+    tests/golden/make_c3_samples.py."""
+    import json
+
     rp, col = B.gen_rmat(22, 28, 0.57, 0.19, 0.19, 11)
     g = B.Graph.from_csr(ctx, rp, col)
     info = g.info()
@@ -348,4 +352,12 @@ def test_c3_k5_sampled_roots(ctx):
     exp = O.count_cliques(rp, col, 5, mod, rem)
     assert got == exp
     assert got > 0
+    with open(os.path.join(ROOT, "tests", "golden", "c3_samples.json")) as f:
+        fx = json.load(f)
+    assert fx["graph"]["m_directed"] == len(col)
+    for smp in fx["samples"]:
+        c, st = B.count_shard(g, P.NAMED[smp["pattern"]], smp["root_rem"], smp["root_mod"], options=B.OPT_TIMING,
+                              stats=True)
+        assert c == smp["count"], smp
+        assert st["roots_large"] >= 1, st
     g.close()

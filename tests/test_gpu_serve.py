@@ -66,3 +66,41 @@ def test_serve_sgc_and_errors(ctx):
     srv.drain()
     srv.close()
     g.close()
+
+
+def test_serve_admission_back_pressure_and_refusal(ctx):
+    """A budget that holds one small request at a time: requests queue behind
+    the batch in flight instead of running out of memory, each result is
+    still exact, and a request whose estimate exceeds the whole budget is
+    refused with BEEP_ERR_OUT_OF_MEMORY."""
+    import torch
+
+    small_rp, small_col = B.gen_erdos_renyi(300, 0.05, 5)
+    hub_rp, hub_col = B.gen_chung_lu(1 << 14, 32.0, 2.1, 9)  # hubs above degree 1024: a large-tier arena
+    assert np.diff(hub_rp).max() > 1024
+    small = B.Graph.from_csr(ctx, small_rp, small_col)
+    hub = B.Graph.from_csr(ctx, hub_rp, hub_col)
+    want = B.count(small, P.TRIANGLE)
+    n, m = len(small_rp) - 1, len(small_col)
+    one = n * 64 + m * 4  # the estimate of one count request on the small graph
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info()
+    srv = B.Server(ctx, max_batch=8, streams=4, hbm_reserve_bytes=free - int(1.5 * one))
+    g_small, g_hub = srv.add_graph(small), srv.add_graph(hub)
+    st0 = srv.stats()
+    assert one <= st0["budget_bytes"] < 2 * one
+    big = srv.submit(g_hub, P.TRIANGLE)
+    rids = [srv.submit(g_small, P.TRIANGLE) for _ in range(20)]
+    with pytest.raises(B.BeepError) as e:
+        srv.wait(big)
+    assert e.value.status == B.ERR_OUT_OF_MEMORY
+    for rid in rids:
+        assert srv.wait(rid)["count"] == want
+    st = srv.stats()
+    assert st["refused"] == 1
+    assert st["requests"] == 20
+    assert st["max_inflight_bytes"] <= st["budget_bytes"]
+    assert st["batches"] == 20  # one request per batch, one batch at a time
+    srv.close()
+    small.close()
+    hub.close()
