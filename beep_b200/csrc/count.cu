@@ -837,29 +837,50 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
     }
     group_sync<G>(gmask);
     const uint32_t T = s_pre[R];
-    for (uint32_t t = tid; t < T; t += nthr) {
-        // row r: last with s_pre[r] <= t
-        uint32_t lo = 0, hi = R;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_pre[mid] <= t)
-                lo = mid;
-            else
-                hi = mid;
+    // kU items per thread per step: their rows are searched and their list
+    // entries loaded before any is searched in A, so a thread keeps kU
+    // independent chains in flight
+    constexpr int kU = 4;
+    for (uint32_t t = tid; t < T; t += nthr * kU) {
+        uint32_t rr[kU], wv[kU];
+#pragma unroll
+        for (int j = 0; j < kU; ++j) {
+            const uint32_t tj = t + nthr * j;
+            rr[j] = 0xffffffffu;
+            wv[j] = 0;
+            if (tj < T) {
+                // row: last with s_pre[r] <= tj
+                uint32_t lo = 0, hi = R;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (s_pre[mid] <= tj)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                rr[j] = lo;
+                if (!(s_len[lo] & kByA))
+                    wv[j] = v.col[s_hb[lo] + (tj - s_pre[lo])];
+            }
         }
-        const uint32_t i = i0 + lo;
-        const uint32_t len = s_len[lo];
-        const uint32_t xb = asc ? max(i + 1, rlo) : 0, xe = asc ? D : i;
-        if (len & kByA) {
-            const uint32_t k = xb + (t - s_pre[lo]);
-            const uint32_t hb = s_hb[lo];
-            if (contains_g(v.col, hb, hb + (len & ~kByA), A[k]))
-                set(i, k);
-        } else {
-            const uint32_t w = v.col[s_hb[lo] + (t - s_pre[lo])];
-            const int k = find_idx(A, xb, xe, w);
-            if (k >= 0)
-                set(i, (uint32_t)k);
+#pragma unroll
+        for (int j = 0; j < kU; ++j) {
+            const uint32_t lo = rr[j];
+            if (lo == 0xffffffffu)
+                continue;
+            const uint32_t i = i0 + lo;
+            const uint32_t len = s_len[lo];
+            const uint32_t xb = asc ? max(i + 1, rlo) : 0, xe = asc ? D : i;
+            if (len & kByA) {
+                const uint32_t k = xb + (t + nthr * j - s_pre[lo]);
+                const uint32_t hb = s_hb[lo];
+                if (contains_g(v.col, hb, hb + (len & ~kByA), A[k]))
+                    set(i, k);
+            } else {
+                const int k = find_idx(A, xb, xe, wv[j]);
+                if (k >= 0)
+                    set(i, (uint32_t)k);
+            }
         }
     }
 }
@@ -966,21 +987,41 @@ __device__ __forceinline__ void build_rows_hashed(const ViewDev &v, int asc, con
         }
         r = lo;
     }
-    for (uint32_t t = t_begin + lane; t < t_end; t += 32) {
-        while (s_pre[r + 1] <= t)
-            ++r;
-        const uint32_t len = s_len[r];
-        const uint32_t xb = asc ? max(r + 1, rlo) : 0, xe = asc ? D : r;
-        const uint32_t off = t - s_pre[r];
-        if (len & kByA) {
-            const uint32_t k = xb + off;
-            const uint32_t hb = s_hb[r];
-            if (contains_g(v.col, hb, hb + (len & ~kByA), A[k]))
-                set(r, k);
-        } else {
-            const int k = hash_find(hkeys, hidx, nslots, hshift, v.col[s_hb[r] + off]);
-            if (k >= (int)xb && k < (int)xe)
-                set(r, (uint32_t)k);
+    // kU items per lane per step: their list entries are loaded before any is
+    // looked up, so a lane keeps kU global loads in flight
+    constexpr int kU = 4;
+    for (uint32_t t = t_begin + lane; t < t_end; t += 32 * kU) {
+        uint32_t rr[kU], wv[kU];
+#pragma unroll
+        for (int j = 0; j < kU; ++j) {
+            const uint32_t tj = t + 32u * j;
+            rr[j] = 0xffffffffu;
+            wv[j] = 0;
+            if (tj < t_end) {
+                while (s_pre[r + 1] <= tj)
+                    ++r;
+                rr[j] = r;
+                if (!(s_len[r] & kByA))
+                    wv[j] = v.col[s_hb[r] + (tj - s_pre[r])];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kU; ++j) {
+            const uint32_t rj = rr[j];
+            if (rj == 0xffffffffu)
+                continue;
+            const uint32_t len = s_len[rj];
+            const uint32_t xb = asc ? max(rj + 1, rlo) : 0, xe = asc ? D : rj;
+            if (len & kByA) {
+                const uint32_t k = xb + (t + 32u * j - s_pre[rj]);
+                const uint32_t hb = s_hb[rj];
+                if (contains_g(v.col, hb, hb + (len & ~kByA), A[k]))
+                    set(rj, k);
+            } else {
+                const int k = hash_find(hkeys, hidx, nslots, hshift, wv[j]);
+                if (k >= (int)xb && k < (int)xe)
+                    set(rj, (uint32_t)k);
+            }
         }
     }
 }
@@ -2097,7 +2138,9 @@ __global__ void __launch_bounds__(256) k_large_nbhd(const PairDev *__restrict__ 
     const int lane = threadIdx.x & 31;
     const uint32_t base0 = bt.tstart[0];
     const uint32_t total = bt.tstart[bt.nb] - base0;
-    uint32_t *la = wsc + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * wstride;
+    // the warp's scratch is shared with k_large_wheel, which needs its first
+    // W words (U) zero on entry: this kernel writes only words [2W, 3W)
+    uint32_t *ws = wsc + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * wstride;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
     int form = kNbNone;
@@ -2136,7 +2179,7 @@ __global__ void __launch_bounds__(256) k_large_nbhd(const PairDev *__restrict__ 
         const uint32_t *deg = rows + nb_deg_offset(D, 0);
         const unsigned long long E = *reinterpret_cast<const unsigned long long *>(rows + nb_edges_offset(D, 0)) / 2;
         const uint32_t u = j0 + (t - bt.tstart[b]);
-        nbhd_task(form, rows, rl, deg, E, W, D, u, t == bt.tstart[b], la, lane, plus, minus);
+        nbhd_task(form, rows, rl, deg, E, W, D, u, t == bt.tstart[b], ws + 2 * (size_t)W, lane, plus, minus);
     }
     plus = warp_sum(plus);
     minus = warp_sum(minus);

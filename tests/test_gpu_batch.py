@@ -104,3 +104,26 @@ def test_tier_limits_and_autotune_keep_counts(ctx):
     batch.close()
     for _, _, g in gs:
         g.close()
+
+
+def test_batch_with_hub_roots_equals_plain_loop(ctx):
+    """A small slice of the batched workload whose graphs have hubs above
+    degree 1,024: every large-tier kernel (walks with donation, the 4-wheel,
+    the neighbourhood statistics) runs in one plan over all 15 central
+    patterns, and each count equals the same pair counted alone."""
+    gs = [B.gen_chung_lu(1 << 14, 32.0, 2.1, 13000 + i) for i in range(3)]
+    assert all(np.diff(rp).max() > 1024 for rp, _ in gs)
+    graphs = [B.Graph.from_csr(ctx, rp, col) for rp, col in gs]
+    pats = P.central_patterns(4) + P.central_patterns(5)
+    batch = B.Batch(ctx)
+    for g in graphs:
+        for q in pats:
+            batch.add(g, q)
+    got, st = batch.run(B.OPT_NO_GRAPH, stats=True)
+    assert st["roots_large"] > 0
+    plain = [B.count(g, q) for g in graphs for q in pats]
+    assert got == plain
+    assert batch.run() == plain  # the captured graph
+    batch.close()
+    for g in graphs:
+        g.close()

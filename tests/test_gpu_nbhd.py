@@ -41,6 +41,19 @@ def hubs(n_leaves, p, seed, n_hubs=2):
     return csr_from_pairs(n_hubs + n_leaves, pairs)
 
 
+def roots_over_hubs(nr, nh, p, seed):
+    """nr roots joined to every one of nh hubs, and G(nh, p) among the hubs:
+    every hub outranks every root, so each root's later neighbours are all nh
+    hubs -- large roots for the forms whose other universal vertices must
+    follow the root (paw, diamond)."""
+    rng = np.random.default_rng(seed)
+    iu = np.triu_indices(nh, 1)
+    m = rng.random(len(iu[0])) < p
+    pairs = list(zip((nr + iu[0][m]).tolist(), (nr + iu[1][m]).tolist()))
+    pairs += [(r, nr + h) for r in range(nr) for h in range(nh)]
+    return csr_from_pairs(nr + nh, pairs)
+
+
 def relabel(q, seed):
     perm = list(range(5))
     random.Random(seed).shuffle(perm)
@@ -55,11 +68,20 @@ def test_forms_are_detected():
                 FORMS.get(i, 0), i
 
 
-def test_forms_match_oracle(ctx):
-    rp, col = hubs(1400, 0.012, 3)
+@pytest.mark.parametrize("graph", ["hubs", "roots_over_hubs"])
+def test_forms_match_oracle(ctx, graph):
+    """Forms whose root has no constraint (wedge, two edges, triangle, path)
+    on hubs of degree 1,400; forms whose other universal vertices follow the
+    root (paw, diamond) on 1,100 roots of degree 1,100 below higher hubs."""
+    if graph == "hubs":
+        rp, col = hubs(1400, 0.012, 3)
+        forms = [6, 7, 9, 10]
+    else:
+        rp, col = roots_over_hubs(1100, 1100, 0.05, 4)
+        forms = [11, 13]
     g = B.Graph.from_csr(ctx, rp, col)
     pats = P.central_patterns(4) + P.central_patterns(5)
-    for i in FORMS:
+    for i in forms:
         for seed in (0, 1):
             q = relabel(pats[i], seed)
             exp = O.count(rp, col, q, apply_root_cap=False)["count"]
@@ -71,16 +93,21 @@ def test_forms_match_oracle(ctx):
 
 
 def test_forms_with_word_lists_match_the_walk(ctx):
-    """Hubs of degree 9,000: rows of 282 words carry non-zero-word lists."""
+    """Hubs of degree 9,000: rows of 282 words carry non-zero-word lists. The
+    batch also holds the 4-wheel, whose kernel shares the per-warp scratch
+    with the statistics kernel and runs after it; each count equals the same
+    pair counted alone."""
     rp, col = hubs(9000, 0.0012, 5, n_hubs=3)
     g = B.Graph.from_csr(ctx, rp, col)
     pats = P.central_patterns(4) + P.central_patterns(5)
+    idx = list(FORMS) + [12]
     b = B.Batch(ctx)
-    for i in FORMS:
+    for i in idx:
         b.add(g, pats[i])
     got = b.run()
     walk = b.run(B.OPT_NO_NBHD | B.OPT_NO_GRAPH)
-    assert got == walk
+    alone = [B.count(g, pats[i]) for i in idx]
+    assert got == walk == alone
     assert all(c > 0 for c in got)
     b.close()
     g.close()

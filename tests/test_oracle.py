@@ -154,6 +154,9 @@ def test_oracle_matches_reference_binary(built, golden):
     # The same sgc diamond run repeated on the mid config: the reference's
     # result changes from run to run (donated subtrees count to full depth
     # while the main path counts prefixes), always between the two counts.
+    # the large config: the reference's bitmap buffer does not fit the device
+    c3 = data["runs"]["c3_rmat_22_28_s11/k5/sgm"]
+    assert c3["returncode"] != 0 and c3["count"] is None and "out of memory" in c3["stderr_tail"]
     reps = data["runs_repeated"]["c2_rmat_20_3_s7/diamond/sgc"]
     counts = golden["large"]["c2_rmat_20_3_s7"]["counts"]["diamond"]
     seen = [r["count"] for r in reps]
