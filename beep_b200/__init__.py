@@ -165,6 +165,9 @@ _SIGNATURES = [
                                              _P(_vp)]),
     ("beep_graph_info_get", ctypes.c_int, [_vp, _P(GraphInfo)]),
     ("beep_graph_csr", ctypes.c_int, [_vp, _P(ctypes.c_int32), _P(ctypes.c_int32)]),
+    ("beep_graph_view", ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32, _P(ctypes.c_int64),
+                                       _P(ctypes.c_int64), _P(ctypes.c_int32), _P(ctypes.c_int32),
+                                       _P(ctypes.c_int32)]),
     ("beep_graph_destroy", ctypes.c_int, [_vp]),
     ("beep_query_load_mtx", ctypes.c_int, [ctypes.c_char_p, _P(_vp)]),
     ("beep_query_from_edges", ctypes.c_int, [ctypes.c_int32, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(_vp)]),
@@ -341,6 +344,20 @@ class Graph:
         ci = np.zeros(max(inf["m"], 1), dtype=np.int32)
         _check(lib().beep_graph_csr(self._h, _i32p(rp), _i32p(ci)))
         return rp, ci[: inf["m"]]
+
+    def view(self, min_qdeg: int, asc: bool = True):
+        """The peeled, priority-relabelled CSR the counting kernels read for
+        this peel threshold and order: (row_ptr, col, orig), orig[i] being
+        the input id of new vertex i."""
+        n, m = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().beep_graph_view(self._h, int(min_qdeg), 1 if asc else 0, ctypes.byref(n), ctypes.byref(m),
+                                     None, None, None))
+        rp = np.zeros(n.value + 1, dtype=np.int32)
+        ci = np.zeros(max(m.value, 1), dtype=np.int32)
+        orig = np.zeros(max(n.value, 1), dtype=np.int32)
+        _check(lib().beep_graph_view(self._h, int(min_qdeg), 1 if asc else 0, ctypes.byref(n), ctypes.byref(m),
+                                     _i32p(rp), _i32p(ci), _i32p(orig)))
+        return rp, ci[: m.value], orig[: n.value]
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -325,6 +325,33 @@ beep_status beep_graph_csr(const beep_graph *g, int32_t *row_ptr, int32_t *col_i
     return BEEP_OK;
 }
 
+beep_status beep_graph_view(beep_graph *g, int32_t min_qdeg, int32_t asc, int64_t *n_out, int64_t *m_out,
+                            int32_t *row_ptr, int32_t *col_ind, int32_t *orig) {
+    if (!g || !n_out || !m_out || min_qdeg < 0)
+        return fail(BEEP_ERR_INVALID_ARG, "beep_graph_view: bad arguments");
+    BEEP_TRY(bind(g->ctx));
+    Ctx *ctx = &g->ctx->impl;
+    std::shared_ptr<View> v;
+    BEEP_TRY(get_view(ctx, &g->impl, min_qdeg, asc ? 1 : 0, false, &v, nullptr));
+    cudaStream_t s = ctx->stream;
+    uint32_t m = 0;
+    BEEP_CUDA_TRY(cudaMemcpyAsync(&m, v->row_ptr.as<uint32_t>() + v->n, 4, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    *n_out = v->n;
+    *m_out = m;
+    if (!row_ptr && !col_ind && !orig)
+        return BEEP_OK;
+    if (!row_ptr || (m > 0 && !col_ind) || (v->n > 0 && !orig))
+        return fail(BEEP_ERR_INVALID_ARG, "beep_graph_view: bad arguments");
+    BEEP_CUDA_TRY(cudaMemcpyAsync(row_ptr, v->row_ptr.ptr, (size_t)(v->n + 1) * 4, cudaMemcpyDeviceToHost, s));
+    if (m > 0)
+        BEEP_CUDA_TRY(cudaMemcpyAsync(col_ind, v->col.ptr, (size_t)m * 4, cudaMemcpyDeviceToHost, s));
+    if (v->n > 0)
+        BEEP_CUDA_TRY(cudaMemcpyAsync(orig, v->orig.ptr, (size_t)v->n * 4, cudaMemcpyDeviceToHost, s));
+    BEEP_CUDA_TRY(cudaStreamSynchronize(s));
+    return BEEP_OK;
+}
+
 beep_status beep_graph_destroy(beep_graph *g) {
     if (g)
         graph_free(g);

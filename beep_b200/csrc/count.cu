@@ -1922,6 +1922,9 @@ __global__ void __launch_bounds__(256) k_large_wheel(const PairDev *__restrict__
     const int lane = threadIdx.x & 31;
     const uint32_t base0 = bt.tstart[0];
     const uint32_t total = bt.tstart[bt.nb] - base0;
+    // three regions of Wm >= every root's W words at fixed places: U (zero
+    // on entry and on exit), U's word list, x1's word list
+    const uint32_t Wm = wstride / 3;
     uint32_t *ws = wsc + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * wstride;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
@@ -1953,7 +1956,7 @@ __global__ void __launch_bounds__(256) k_large_wheel(const PairDev *__restrict__
         rl.cap = list_cap(W);
         rl.nzc = rows + (size_t)D * W;
         rl.nzl = rl.nzc + D;
-        wheel4_task(rows, rl, W, j0 + (t - bt.tstart[b]), ws, ws + W, ws + 2 * (size_t)W, lane, cnt);
+        wheel4_task(rows, rl, W, j0 + (t - bt.tstart[b]), ws, ws + Wm, ws + 2 * (size_t)Wm, lane, cnt);
     }
     cnt = warp_sum(cnt);
     if (lane == 0)
@@ -2139,7 +2142,9 @@ __global__ void __launch_bounds__(256) k_large_nbhd(const PairDev *__restrict__ 
     const uint32_t base0 = bt.tstart[0];
     const uint32_t total = bt.tstart[bt.nb] - base0;
     // the warp's scratch is shared with k_large_wheel, which needs its first
-    // W words (U) zero on entry: this kernel writes only words [2W, 3W)
+    // wstride / 3 words (U, for roots of any width) zero on entry: this
+    // kernel writes only the third region, words [2 Wm, 3 Wm)
+    const uint32_t Wm = wstride / 3;
     uint32_t *ws = wsc + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * wstride;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
@@ -2179,7 +2184,7 @@ __global__ void __launch_bounds__(256) k_large_nbhd(const PairDev *__restrict__ 
         const uint32_t *deg = rows + nb_deg_offset(D, 0);
         const unsigned long long E = *reinterpret_cast<const unsigned long long *>(rows + nb_edges_offset(D, 0)) / 2;
         const uint32_t u = j0 + (t - bt.tstart[b]);
-        nbhd_task(form, rows, rl, deg, E, W, D, u, t == bt.tstart[b], ws + 2 * (size_t)W, lane, plus, minus);
+        nbhd_task(form, rows, rl, deg, E, W, D, u, t == bt.tstart[b], ws + 2 * (size_t)Wm, lane, plus, minus);
     }
     plus = warp_sum(plus);
     minus = warp_sum(minus);

@@ -250,14 +250,34 @@ __global__ void k_peel_fused(const uint32_t *__restrict__ rp, const uint32_t *__
 
 // ---- relabelling -----------------------------------------------------------
 
+// Row classes of the relabelled CSR (see the relabelled rows below).
+constexpr int kRowClasses = 11;     // lengths 1, 2, 3-4, .., 129-256, 257-kHubTile, longer
+constexpr uint32_t kHubTile = 4096; // entries of a hub tile (and of a block sort)
+// vstat words: [0, kRowClasses) rows per class, then the hub tiles, the most
+// tiles of one hub row and the peel rounds
+constexpr int kVsTiles = kRowClasses, kVsMaxTiles = kRowClasses + 1, kVsRounds = kRowClasses + 2;
+constexpr int kVsWords = 16;
+
+__device__ __forceinline__ int row_class(uint32_t d) {
+    if (d <= 1)
+        return 0;
+    if (d <= 256)
+        return 32 - __clz((int)(d - 1)); // 2 -> 1, 3..4 -> 2, .., 129..256 -> 8
+    return d <= kHubTile ? 9 : 10;
+}
+
 // Priority key (subgraph_matching.cuh:1299-1331, host_utils.cuh:230-246):
 // ascending (degree, id) or descending degree with ties by ascending id.
 // Vertices left with no edge get the largest key and are dropped.
 // The key is the degree part alone; a stable radix sort of (key, id) pairs
 // with ids in increasing order keeps ties by ascending id.
+// vstat gets the kept vertices per row class and the hub tile counts.
 __global__ void k_prio_keys(const uint32_t *__restrict__ deg, int64_t n, uint32_t maxdeg, int asc,
-                            uint32_t *keys, uint32_t *ids, unsigned long long *n_alive) {
-    unsigned long long c = 0;
+                            uint32_t *keys, uint32_t *ids, uint32_t *vstat) {
+    __shared__ uint32_t hist[kRowClasses + 2];
+    if (threadIdx.x < kRowClasses + 2)
+        hist[threadIdx.x] = 0;
+    __syncthreads();
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t d = deg[v];
         uint32_t k;
@@ -265,15 +285,22 @@ __global__ void k_prio_keys(const uint32_t *__restrict__ deg, int64_t n, uint32_
             k = maxdeg;
         } else {
             k = asc ? d - 1 : maxdeg - d;
-            ++c;
+            const int c = row_class(d);
+            atomicAdd(&hist[c], 1u);
+            if (c == kRowClasses - 1) {
+                const uint32_t t = (d + kHubTile - 1) / kHubTile;
+                atomicAdd(&hist[kVsTiles], t);
+                atomicMax(&hist[kVsMaxTiles], t);
+            }
         }
         keys[v] = k;
         ids[v] = (uint32_t)v;
     }
-    for (int o = 16; o > 0; o >>= 1)
-        c += __shfl_xor_sync(kFull, c, o);
-    if ((threadIdx.x & 31) == 0 && c)
-        atomicAdd(n_alive, c);
+    __syncthreads();
+    if (threadIdx.x < kRowClasses + 1 && hist[threadIdx.x])
+        atomicAdd(&vstat[threadIdx.x], hist[threadIdx.x]);
+    if (threadIdx.x == kVsMaxTiles && hist[threadIdx.x])
+        atomicMax(&vstat[threadIdx.x], hist[threadIdx.x]);
 }
 
 __global__ void k_rank(const uint32_t *__restrict__ sorted_ids, int64_t n_alive, uint32_t *orig, uint32_t *rank,
@@ -287,62 +314,305 @@ __global__ void k_rank(const uint32_t *__restrict__ sorted_ids, int64_t n_alive,
     }
 }
 
-// The relabelled rows are produced by one sort: every input entry (v, w)
-// becomes the key (rank v) << rb | rank w (ranks < 2^rb), or ~0 when either
-// end was dropped,
-// written at the entry's own position; sorting the keys leaves the new rows
-// in order, each sorted, with the dropped entries after them. No per-row
-// sort, so a few very long rows (hubs) cannot hold up the rest.
-__device__ __forceinline__ uint64_t view_key(uint32_t rv, uint32_t rw, int rb) {
-    return (rv == 0xffffffffu || rw == 0xffffffffu) ? ~0ull : (((uint64_t)rv << rb) | rw);
+// ---- relabelled rows --------------------------------------------------------
+//
+// New row j (input vertex v = orig[j]) holds rank[w] for every surviving
+// neighbour w of v, in increasing order. Its length is v's degree after the
+// peel, so the priority order makes the lengths monotone in j (rising for the
+// ascending order, falling for the descending one) and every size class
+// below is one contiguous range of rows. The rows are built in two steps:
+// a gather that writes each row's entries, unordered, at its final place,
+// then a sort of each row inside its own range, by size class: bitonic
+// networks over 2..32 lanes of a warp (shuffles), over a warp's shared
+// memory (up to 256 entries) or a block's (up to kHubTile), and for longer
+// rows (hubs) sorted tiles of kHubTile entries merged in passes that all
+// blocks of the GPU share.
+// First row of class c and the rows it holds, from the class counts.
+__device__ __forceinline__ uint32_t class_first(const uint32_t *cnt, int c, int asc) {
+    uint32_t f = 0;
+    for (int i = 0; i < kRowClasses; ++i)
+        if (asc ? i < c : i > c)
+            f += cnt[i];
+    return f;
 }
 
-__global__ void k_fill_keys(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
-                            const uint32_t *__restrict__ rank, int64_t n, int rb, uint64_t *keys,
-                            RowChunk *chunks, unsigned *n_chunks, uint32_t cap) {
+// Input row v's surviving entries, as new ids, at new row rank[v]'s place:
+// rows of up to kSerialMax entries by one lane each, longer rows by chunks
+// (k_view_fill_chunks) that reserve their part of the row with an atomic on
+// the row's cursor.
+__global__ void k_view_fill(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col,
+                            const uint32_t *__restrict__ rank, int64_t n, const uint32_t *__restrict__ nrp,
+                            uint32_t *vcol, RowChunk *chunks, unsigned *n_chunks, uint32_t cap) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += warps * 32) {
         const int64_t v = base + lane;
         bool big = false;
-        uint32_t b = 0, e = 0;
+        uint32_t b = 0, e = 0, rv = 0;
         if (v < n) {
-            b = rp[v];
-            e = rp[v + 1];
-            if (e - b > kSerialMax) {
-                big = true;
-            } else {
-                const uint32_t rv = rank[v];
-                for (uint32_t k = b; k < e; ++k)
-                    keys[k] = view_key(rv, rank[col[k]], rb);
+            rv = rank[v];
+            if (rv != 0xffffffffu) {
+                b = rp[v];
+                e = rp[v + 1];
+                if (e - b > kSerialMax) {
+                    big = true;
+                } else {
+                    uint32_t o = nrp[rv];
+#pragma unroll 4
+                    for (uint32_t k = b; k < e; ++k) {
+                        const uint32_t r = rank[col[k]];
+                        if (r != 0xffffffffu)
+                            vcol[o++] = r;
+                    }
+                }
             }
         }
-        push_chunks(big, (uint32_t)v, b, e, chunks, n_chunks, cap, lane);
+        push_chunks(big, rv, b, e, chunks, n_chunks, cap, lane);
     }
 }
 
-__global__ void k_fill_key_chunks(const uint32_t *__restrict__ col, const uint32_t *__restrict__ rank,
-                                  const RowChunk *__restrict__ chunks, const unsigned *__restrict__ n_chunks,
-                                  uint32_t cap, int rb, uint64_t *keys) {
+// A warp per chunk of kChunk = 32 x 32 entries: all loads first, then one
+// atomic for the chunk's survivors, then the compacted stores.
+__global__ void k_view_fill_chunks(const uint32_t *__restrict__ col, const uint32_t *__restrict__ rank,
+                                   const RowChunk *__restrict__ chunks, const unsigned *__restrict__ n_chunks,
+                                   uint32_t cap, const uint32_t *__restrict__ nrp, uint32_t *cur, uint32_t *vcol) {
+    static_assert(kChunk == 32 * 32, "a lane holds kChunk / 32 entries");
     const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t nc = min(*n_chunks, cap);
     for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc; c += warps) {
         const RowChunk ch = chunks[c];
-        const uint32_t rv = rank[ch.row];
-        for (uint32_t k = ch.b + lane; k < ch.e; k += 32)
-            keys[k] = view_key(rv, rank[col[k]], rb);
+        uint32_t r[32];
+        uint32_t tot = 0;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            const uint32_t k = ch.b + (uint32_t)(i * 32 + lane);
+            r[i] = k < ch.e ? rank[col[k]] : 0xffffffffu;
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            tot += (uint32_t)__popc(__ballot_sync(kFull, r[i] != 0xffffffffu));
+        uint32_t o = 0;
+        if (lane == 0 && tot)
+            o = atomicAdd(&cur[ch.row], tot);
+        o = nrp[ch.row] + __shfl_sync(kFull, o, 0);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            const unsigned bal = __ballot_sync(kFull, r[i] != 0xffffffffu);
+            if (r[i] != 0xffffffffu)
+                vcol[o + (uint32_t)__popc(bal & lt)] = r[i];
+            o += (uint32_t)__popc(bal);
+        }
     }
 }
 
-// The first *m_live sorted keys are the view's entries (the dropped ones,
-// all ones, sort last).
-__global__ void k_keys_low(const uint64_t *__restrict__ keys, const uint32_t *__restrict__ m_live, int rb,
-                           uint32_t *col) {
-    const uint64_t mask = ((uint64_t)1 << rb) - 1;
-    const int64_t m = *m_live;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
-        col[i] = (uint32_t)(keys[i] & mask);
+// Hub row h (new row h0 + h): its tile count, at htp[h + 1] (a scan turns
+// them into each hub's first tile).
+__global__ void k_hub_tiles(const uint32_t *__restrict__ nrp, uint32_t h0, uint32_t H, uint32_t *htp) {
+    for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < H; h += gridDim.x * blockDim.x)
+        htp[h + 1] = (nrp[h0 + h + 1] - nrp[h0 + h] + kHubTile - 1) / kHubTile;
+}
+
+// last h with htp[h] <= u (htp rising, htp[0] = 0 <= u)
+__device__ __forceinline__ uint32_t hub_of(const uint32_t *__restrict__ htp, uint32_t H, uint32_t u) {
+    uint32_t lo = 0, hi = H;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (htp[mid] <= u)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Bitonic sort, ascending, of s[0, S) (S a power of two) by `nt` threads
+// numbered `t`; `sync` separates the stages.
+template <typename Sync>
+__device__ __forceinline__ void bitonic_shared(uint32_t *s, uint32_t S, uint32_t t, uint32_t nt, Sync sync) {
+    for (uint32_t k = 2; k <= S; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t q = t; q < S / 2; q += nt) {
+                const uint32_t i = 2 * q - (q & (j - 1)), l = i + j;
+                const uint32_t a = s[i], b = s[l];
+                if ((a > b) == ((i & k) == 0)) {
+                    s[i] = b;
+                    s[l] = a;
+                }
+            }
+            sync();
+        }
+}
+
+// One unit of the row sort: class c's rows [first, first + cnt) in units of
+// (256 >> c) rows (c <= 5: a group of 2^c lanes per row), 8 rows (c = 6..8:
+// a warp per row), one row (c = 9) or one hub tile (c = 10). Units are taken
+// longest class first from a cursor, so the hubs' tiles start at once.
+// Hub tiles go to out[]: the buffer that, after the merge passes, leaves the
+// hub rows in vcol.
+__global__ void __launch_bounds__(256) k_view_sort(const uint32_t *__restrict__ nrp, const uint32_t *__restrict__ vstat,
+                                                   int asc, const uint32_t *__restrict__ htp, uint32_t *vcol,
+                                                   uint32_t *out, unsigned *cursor) {
+    __shared__ uint32_t buf[kHubTile];
+    __shared__ uint32_t s_first[kRowClasses], s_cnt[kRowClasses], s_ustart[kRowClasses + 1];
+    __shared__ uint32_t s_u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        uint32_t cnt[kRowClasses];
+        for (int c = 0; c < kRowClasses; ++c)
+            cnt[c] = vstat[c];
+        uint32_t acc = 0;
+        for (int c = kRowClasses - 1; c >= 0; --c) {
+            s_first[c] = class_first(cnt, c, asc);
+            s_cnt[c] = cnt[c];
+            s_ustart[c] = acc;
+            uint32_t units = 0;
+            if (c == 10)
+                units = vstat[kVsTiles];
+            else if (c == 9)
+                units = cnt[c];
+            else if (c >= 6)
+                units = (cnt[c] + 7) / 8;
+            else if (c >= 1)
+                units = (cnt[c] + (256u >> c) - 1) / (256u >> c);
+            acc += units;
+        }
+        s_ustart[kRowClasses] = acc; // total
+    }
+    __syncthreads();
+    const uint32_t total = s_ustart[kRowClasses];
+    for (;;) {
+        if (threadIdx.x == 0)
+            s_u = atomicAdd(cursor, 1u);
+        __syncthreads();
+        const uint32_t u = s_u;
+        __syncthreads();
+        if (u >= total)
+            break;
+        int c = kRowClasses - 1; // classes hold units in falling order
+        while (c > 0 && u >= s_ustart[c - 1])
+            --c;
+        const uint32_t lu = u - s_ustart[c];
+        const uint32_t first = s_first[c], cend = first + s_cnt[c];
+        if (c >= 9) {
+            uint32_t j, lo, len;
+            uint32_t *dst = vcol;
+            if (c == 10) {
+                const uint32_t H = s_cnt[10];
+                const uint32_t h = hub_of(htp, H, lu);
+                j = first + h;
+                lo = nrp[j] + (lu - htp[h]) * kHubTile;
+                len = min(kHubTile, nrp[j + 1] - lo);
+                dst = out;
+            } else {
+                j = first + lu;
+                lo = nrp[j];
+                len = nrp[j + 1] - lo;
+            }
+            uint32_t S = 512;
+            while (S < len)
+                S <<= 1;
+            for (uint32_t i = threadIdx.x; i < S; i += blockDim.x)
+                buf[i] = i < len ? vcol[lo + i] : 0xffffffffu;
+            __syncthreads();
+            bitonic_shared(buf, S, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+            for (uint32_t i = threadIdx.x; i < len; i += blockDim.x)
+                dst[lo + i] = buf[i];
+            __syncthreads();
+        } else if (c >= 6) {
+            const uint32_t j = first + lu * 8 + (uint32_t)warp;
+            if (j < cend) {
+                const uint32_t S = 1u << c, lo = nrp[j], len = nrp[j + 1] - lo;
+                uint32_t *s = buf + warp * 256;
+                for (uint32_t i = lane; i < S; i += 32)
+                    s[i] = i < len ? vcol[lo + i] : 0xffffffffu;
+                __syncwarp();
+                bitonic_shared(s, S, lane, 32, [] { __syncwarp(); });
+                for (uint32_t i = lane; i < len; i += 32)
+                    vcol[lo + i] = s[i];
+            }
+        } else if (c >= 1) {
+            // groups of P = 2^c lanes, a row each
+            const uint32_t P = 1u << c, g = (uint32_t)lane >> c, i = (uint32_t)lane & (P - 1);
+            const uint32_t j = first + lu * (256u >> c) + (uint32_t)warp * (32u >> c) + g;
+            uint32_t lo = 0, len = 0;
+            if (j < cend) {
+                lo = nrp[j];
+                len = nrp[j + 1] - lo;
+            }
+            uint32_t x = i < len ? vcol[lo + i] : 0xffffffffu;
+            for (uint32_t k = 2; k <= P; k <<= 1)
+                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+                    const uint32_t y = __shfl_xor_sync(kFull, x, (int)jj);
+                    const bool keep_min = ((i & jj) == 0) == ((i & k) == 0);
+                    x = keep_min ? min(x, y) : max(x, y);
+                }
+            if (i < len)
+                vcol[lo + i] = x;
+        }
+    }
+}
+
+// Merge-path split: how many of A's entries are among the first d of the
+// merge of A (na) and B (nb); entries are distinct.
+__device__ __forceinline__ uint32_t merge_split(const uint32_t *A, uint32_t na, const uint32_t *B, uint32_t nb,
+                                                uint32_t d) {
+    uint32_t lo = d > nb ? d - nb : 0u, hi = min(d, na);
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (A[mid] < B[d - 1 - mid])
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Merge pass p over the hub rows: sorted runs of kHubTile << p entries are
+// merged in pairs, src -> dst. Unit u is output window u - htp[h] (kHubTile
+// entries) of hub h: its parts of the two runs are found by a merge-path
+// search, staged in shared memory, and every thread merges 16 outputs. A run
+// without a partner is copied.
+__global__ void __launch_bounds__(256) k_view_merge(const uint32_t *__restrict__ nrp, uint32_t h0, uint32_t H,
+                                                    const uint32_t *__restrict__ htp, int p,
+                                                    const uint32_t *__restrict__ src, uint32_t *dst) {
+    __shared__ uint32_t sm[kHubTile];
+    __shared__ uint32_t s_split[2];
+    static_assert(kHubTile == 256 * 16, "16 outputs a thread");
+    const uint32_t TT = htp[H];
+    for (uint32_t u = blockIdx.x; u < TT; u += gridDim.x) {
+        const uint32_t h = hub_of(htp, H, u), w = u - htp[h];
+        const uint32_t rb = nrp[h0 + h], L = nrp[h0 + h + 1] - rb;
+        const uint64_t R = (uint64_t)kHubTile << p;
+        const uint64_t ps = (uint64_t)(w >> (p + 1)) * 2 * R; // the pair's first entry
+        const uint64_t left = (uint64_t)L - ps; // entries from the pair's first on (> 0)
+        const uint32_t al = (uint32_t)(left < R ? left : R);
+        const uint32_t bl = (uint32_t)(left - al < R ? left - al : R);
+        const uint32_t d0 = (uint32_t)((uint64_t)w * kHubTile - ps), d1 = min(d0 + kHubTile, al + bl);
+        const uint32_t *A = src + rb + ps, *B = A + al;
+        if (threadIdx.x < 2)
+            s_split[threadIdx.x] = merge_split(A, al, B, bl, threadIdx.x ? d1 : d0);
+        __syncthreads();
+        const uint32_t a0 = s_split[0], a1 = s_split[1], b0 = d0 - a0, b1 = d1 - a1;
+        const uint32_t na = a1 - a0, nb = b1 - b0;
+        for (uint32_t i = threadIdx.x; i < na; i += blockDim.x)
+            sm[i] = A[a0 + i];
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x)
+            sm[na + i] = B[b0 + i];
+        __syncthreads();
+        const uint32_t n = na + nb, dd = threadIdx.x * 16;
+        if (dd < n) {
+            const uint32_t de = min(dd + 16, n);
+            uint32_t ai = merge_split(sm, na, sm + na, nb, dd), bi = dd - ai;
+            uint32_t *o = dst + rb + ps + d0;
+            for (uint32_t q = dd; q < de; ++q) {
+                const bool take_a = bi >= nb || (ai < na && sm[ai] < sm[na + bi]);
+                o[q] = take_a ? sm[ai++] : sm[na + bi++];
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // split[i] = number of neighbours with a smaller new id (lower_bound of i).
@@ -576,8 +846,8 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     const size_t cap = chunk_capacity(n, m);
     const size_t mm = m > 0 ? (size_t)m : 1;
     size_t need = Carve::need({(size_t)nn * 4, (size_t)nn, (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4,
-                               (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4, mm * 8, mm * 8,
-                               cap * sizeof(RowChunk), 16, (size_t)nn * 4, kPeelMaxRounds * 8});
+                               (size_t)nn * 4, (size_t)nn * 4, (size_t)nn * 4, mm * 4, cap * sizeof(RowChunk), 16,
+                               (size_t)nn * 4, kPeelMaxRounds * 8, kVsWords * 4, ((size_t)nn + 1) * 4});
     BEEP_TRY(ctx->grow(ctx->scratch2, need));
     Carve cv(ctx->scratch2.ptr);
     uint32_t *deg = cv.take<uint32_t>(nn);
@@ -586,14 +856,14 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     uint32_t *pkey = cv.take<uint32_t>(nn), *pid = cv.take<uint32_t>(nn);
     uint32_t *pkey2 = cv.take<uint32_t>(nn), *pid2 = cv.take<uint32_t>(nn);
     uint32_t *new_deg = cv.take<uint32_t>(nn);
-    uint64_t *ekeys = cv.take<uint64_t>(mm), *ekeys2 = cv.take<uint64_t>(mm);
+    uint32_t *hub_tmp = cv.take<uint32_t>(mm); // the hub rows' other merge buffer
     RowChunk *chunks = cv.take<RowChunk>(cap);
-    unsigned *d_nchunks = cv.take<unsigned>(4); // [0] chunk count, [2] peel rounds
+    unsigned *d_nchunks = cv.take<unsigned>(4); // [0] chunk count, [1] row sort cursor
     uint32_t *peel_list = cv.take<uint32_t>(nn);
     unsigned long long *peel_removed = cv.take<unsigned long long>(kPeelMaxRounds);
+    uint32_t *vstat = cv.take<uint32_t>(kVsWords);
+    uint32_t *htp = cv.take<uint32_t>((size_t)nn + 1); // first tile of every hub row
     const uint32_t ucap = (uint32_t)std::min<size_t>(cap, 0xffffffffu);
-    BEEP_TRY(ctx->grow(ctx->counter, 64));
-    unsigned long long *d_removed = ctx->counter.as<unsigned long long>();
 
     PhaseTrace tr("view", s);
     const int gv = grid_for(n, 256, ctx->num_sms);
@@ -604,8 +874,8 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_CUDA_TRY(cudaGetLastError());
     // Iterated peel, all rounds in one cooperative launch (no host round trip
     // per round).
-    int *d_rounds = reinterpret_cast<int *>(d_nchunks + 2);
-    BEEP_CUDA_TRY(cudaMemsetAsync(d_rounds, 0, 4, s));
+    BEEP_CUDA_TRY(cudaMemsetAsync(vstat, 0, kVsWords * 4, s));
+    int *d_rounds = reinterpret_cast<int *>(vstat + kVsRounds);
     if (min_qdeg > 1 && n > 0) {
         BEEP_CUDA_TRY(cudaMemsetAsync(peel_removed, 0, kPeelMaxRounds * 8, s));
         int per_sm = 0;
@@ -628,10 +898,8 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     int hb = 1;
     while (hb < 32 && ((uint64_t)1 << hb) <= (uint64_t)maxdeg)
         ++hb;
-    unsigned long long *d_alive = d_removed + 1;
-    BEEP_CUDA_TRY(cudaMemsetAsync(d_alive, 0, 8, s));
     if (n > 0) {
-        k_prio_keys<<<gv, 256, 0, s>>>(deg, n, maxdeg, asc, pkey, pid, d_alive);
+        k_prio_keys<<<gv, 256, 0, s>>>(deg, n, maxdeg, asc, pkey, pid, vstat);
         ++ctx->launches;
     }
     BEEP_CUDA_TRY(cudaGetLastError());
@@ -639,14 +907,21 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, pkey, pkey2, pid, pid2, n, 0, hb, s));
     BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
     BEEP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ctx->scratch.ptr, tb, pkey, pkey2, pid, pid2, n, 0, hb, s));
-    // number of vertices that kept an edge
-    ctx->h_pinned[1] = 0; // the copy below fills its low 4 bytes
-    BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, d_alive, 8, cudaMemcpyDeviceToHost, s));
-    BEEP_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned + 1, d_rounds, 4, cudaMemcpyDeviceToHost, s));
+    // rows per class (their sum: the vertices that kept an edge), hub tiles,
+    // peel rounds
+    static_assert(kVsWords * 4 <= 64, "the pinned mirror holds 64 bytes");
+    uint32_t *hv = reinterpret_cast<uint32_t *>(ctx->h_pinned);
+    BEEP_CUDA_TRY(cudaMemcpyAsync(hv, vstat, kVsWords * 4, cudaMemcpyDeviceToHost, s));
     BEEP_CUDA_TRY(cudaStreamSynchronize(s));
-    const int64_t na = (int64_t)ctx->h_pinned[0];
+    uint32_t cls[kRowClasses];
+    int64_t na = 0;
+    for (int c = 0; c < kRowClasses; ++c) {
+        cls[c] = hv[c];
+        na += cls[c];
+    }
+    const uint32_t hub_tiles = hv[kVsTiles], hub_max_tiles = hv[kVsMaxTiles];
     v->n = na;
-    v->peel_rounds = std::max(1, (int)(uint32_t)ctx->h_pinned[1]);
+    v->peel_rounds = std::max(1, (int)hv[kVsRounds]);
     tr.mark("order");
     BEEP_TRY(ctx->grow(v->row_ptr, (size_t)(na + 1) * 4));
     BEEP_TRY(ctx->grow(v->orig, (size_t)(na > 0 ? na : 1) * 4));
@@ -668,34 +943,64 @@ beep_status build_view(Ctx *ctx, Graph *g, int32_t min_qdeg, int32_t asc, View *
     // sized for all m input entries and the kernels read the count there.
     tr.mark("rank_scan");
     BEEP_TRY(ctx->grow(v->col, (size_t)(m > 0 ? m : 1) * 4));
-    // rank bits: every rank is below na < 2^rb
-    int rb = 1;
-    while (rb < 32 && ((uint64_t)1 << rb) <= (uint64_t)na)
-        ++rb;
+    uint32_t *vcol = v->col.as<uint32_t>();
     if (m > 0 && na > 0) {
-        BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks, 0, 4, s));
-        k_fill_keys<<<gv, 256, 0, s>>>(rp, col, rank, n, rb, ekeys, chunks, d_nchunks, ucap);
-        k_fill_key_chunks<<<ctx->num_sms * 8, 256, 0, s>>>(col, rank, chunks, d_nchunks, ucap, rb, ekeys);
+        // new_deg is free after the scan: the long rows' fill cursors
+        BEEP_CUDA_TRY(cudaMemsetAsync(new_deg, 0, (size_t)na * 4, s));
+        BEEP_CUDA_TRY(cudaMemsetAsync(d_nchunks, 0, 8, s));
+        k_view_fill<<<gv, 256, 0, s>>>(rp, col, rank, n, nrp, vcol, chunks, d_nchunks, ucap);
+        k_view_fill_chunks<<<ctx->num_sms * 8, 256, 0, s>>>(col, rank, chunks, d_nchunks, ucap, nrp, new_deg, vcol);
         ctx->launches += 2;
         BEEP_CUDA_TRY(cudaGetLastError());
     }
     tr.mark("fill");
     if (m > 0 && na > 0) {
-        tb = 0;
-        BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, ekeys, ekeys2, m, 0, 2 * rb, s));
-        BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
-        BEEP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(ctx->scratch.ptr, tb, ekeys, ekeys2, m, 0, 2 * rb, s));
-        k_keys_low<<<grid_for(m, 256, ctx->num_sms), 256, 0, s>>>(ekeys2, nrp + na, rb, v->col.as<uint32_t>());
-        ++ctx->launches;
-        BEEP_CUDA_TRY(cudaGetLastError());
+        // hub rows: [h0, h0 + H) of the new order; their tiles go through
+        // `passes` merges, so the tile sort writes them where the last
+        // merge pass leaves them in vcol
+        const uint32_t H = cls[kRowClasses - 1];
+        const uint32_t h0 = asc ? (uint32_t)(na - H) : 0u;
+        int passes = 0;
+        while (((uint32_t)1 << passes) < hub_max_tiles)
+            ++passes;
+        uint32_t *bufs[2] = {vcol, hub_tmp};
+        if (H > 0) {
+            BEEP_CUDA_TRY(cudaMemsetAsync(htp, 0, 4, s));
+            k_hub_tiles<<<grid_for(H, 256, ctx->num_sms), 256, 0, s>>>(nrp, h0, H, htp);
+            ++ctx->launches;
+            BEEP_CUDA_TRY(cudaGetLastError());
+            tb = 0;
+            BEEP_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb, htp + 1, htp + 1, H, s));
+            BEEP_TRY(ctx->grow(ctx->scratch, tb + 1024));
+            BEEP_CUDA_TRY(cub::DeviceScan::InclusiveSum(ctx->scratch.ptr, tb, htp + 1, htp + 1, H, s));
+        }
+        uint64_t units = hub_tiles + cls[9];
+        for (int c = 1; c <= 8; ++c)
+            units += c >= 6 ? (cls[c] + 7) / 8 : (cls[c] + (256u >> c) - 1) / (256u >> c);
+        if (units > 0) {
+            int per_sm = 0;
+            BEEP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_view_sort, 256, 0));
+            const int64_t blocks = std::min<int64_t>((int64_t)std::max(per_sm, 1) * ctx->num_sms, (int64_t)units);
+            k_view_sort<<<(unsigned)blocks, 256, 0, s>>>(nrp, vstat, asc, htp, vcol, bufs[passes & 1],
+                                                         d_nchunks + 1);
+            ++ctx->launches;
+            BEEP_CUDA_TRY(cudaGetLastError());
+        }
+        const unsigned mgrid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(hub_tiles, ctx->num_sms * 8ull));
+        for (int p = 0; p < passes; ++p) {
+            k_view_merge<<<mgrid, 256, 0, s>>>(nrp, h0, H, htp, p, bufs[(passes - p) & 1],
+                                               bufs[(passes - p - 1) & 1]);
+            ++ctx->launches;
+            BEEP_CUDA_TRY(cudaGetLastError());
+        }
     }
+    tr.mark("sort");
     if (na > 0) {
-        k_split<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(nrp, v->col.as<uint32_t>(), na,
-                                                                v->split.as<uint32_t>());
+        k_split<<<grid_for(na, 256, ctx->num_sms), 256, 0, s>>>(nrp, vcol, na, v->split.as<uint32_t>());
         ++ctx->launches;
     }
     BEEP_CUDA_TRY(cudaGetLastError());
-    tr.mark("sort_split");
+    tr.mark("split");
     return BEEP_OK;
 }
 

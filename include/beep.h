@@ -122,6 +122,16 @@ typedef struct beep_graph_info {
 beep_status beep_graph_info_get(const beep_graph *g, beep_graph_info *out);
 /* Copy the deduped CSR back to the host (row_ptr[n+1], col_ind[m]). */
 beep_status beep_graph_csr(const beep_graph *g, int32_t *row_ptr, int32_t *col_ind);
+/* The graph as the counting kernels read it for one peel threshold and order
+ * (built and cached as a count would): the iterated peel of the vertices of
+ * degree in [1, min_qdeg) (subgraph_matching.cuh:685-764), then every vertex
+ * that kept an edge, in priority order -- ascending (degree, id) when asc,
+ * else descending degree with ties by ascending id -- and each row the sorted
+ * new ids of its surviving neighbours (subgraph_matching.cuh:1282-1336).
+ * With NULL arrays only *n_out and *m_out are written; otherwise row_ptr[n+1],
+ * col_ind[m] and orig[n] (the input id of every new vertex) are filled too. */
+beep_status beep_graph_view(beep_graph *g, int32_t min_qdeg, int32_t asc, int64_t *n_out, int64_t *m_out,
+                            int32_t *row_ptr, int32_t *col_ind, int32_t *orig);
 beep_status beep_graph_destroy(beep_graph *g);
 
 /* ---- query ------------------------------------------------------------- */

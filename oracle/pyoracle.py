@@ -204,6 +204,29 @@ def peel(row_ptr, col, min_qdeg):
     return deg[:n], alive[:n].astype(bool), rounds
 
 
+def view(row_ptr, col, min_qdeg, asc=True):
+    """The peeled, priority-relabelled CSR: or_peel, then every vertex that
+    kept an edge in build_rank's order (ascending (degree, id), or descending
+    degree with ties by ascending id; subgraph_matching.cuh:1282-1336,
+    host_utils.cuh:230-246) and each row the sorted new ids of its kept
+    neighbours. Returns int32 (row_ptr, col, orig)."""
+    deg, keep, _ = peel(row_ptr, col, min_qdeg)
+    rp = np.asarray(row_ptr, dtype=np.int64)
+    c = np.asarray(col, dtype=np.int64)
+    n = len(rp) - 1
+    ids = np.nonzero(keep)[0].astype(np.int64)
+    d = deg[ids].astype(np.int64)
+    orig = ids[np.lexsort((ids, d if asc else -d))]
+    rank = np.full(max(n, 1), -1, dtype=np.int64)
+    rank[orig] = np.arange(len(orig), dtype=np.int64)
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp))
+    ok = (rank[src] >= 0) & (rank[c] >= 0)
+    keys = np.sort((rank[src][ok] << np.int64(32)) | rank[c][ok])
+    nrp = np.zeros(len(orig) + 1, dtype=np.int64)
+    nrp[1:] = np.cumsum(np.bincount(keys >> np.int64(32), minlength=len(orig)))
+    return nrp.astype(np.int32), (keys & np.int64(0xFFFFFFFF)).astype(np.int32), orig.astype(np.int32)
+
+
 def cutoff(row_ptr) -> int:
     rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
     return int(lib().or_cutoff(len(rp) - 1, _i64p(rp)))

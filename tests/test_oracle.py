@@ -186,3 +186,21 @@ def test_non_central_golden_and_closed_forms(built):
         rp, col = gens[rec["kind"]](*rec["args"])
         for pname, c in rec["counts"].items():
             assert O.brute_force(rp, col, P.NON_CENTRAL[pname]) == c, (gname, pname)
+
+
+def test_oracle_view_matches_loops():
+    """The oracle's relabelled CSR against plain loops: peel, order the kept
+    vertices by (degree, id) or (-degree, id), sort each row's new ids."""
+    from oracle import synth
+
+    rp, col = synth.erdos_renyi(300, 0.03, 4)
+    for min_qdeg in (1, 3, 6):
+        deg, keep, _ = O.peel(rp, col, min_qdeg)
+        for asc in (True, False):
+            kept = [v for v in range(len(rp) - 1) if keep[v]]
+            kept.sort(key=lambda v: ((deg[v] if asc else -deg[v]), v))
+            rank = {v: i for i, v in enumerate(kept)}
+            rows = [sorted(rank[w] for w in col[rp[v]:rp[v + 1]] if w in rank) for v in kept]
+            nrp, c, orig = O.view(rp, col, min_qdeg, asc)
+            assert list(orig) == kept
+            assert [list(c[nrp[i]:nrp[i + 1]]) for i in range(len(kept))] == rows
