@@ -33,6 +33,7 @@
 // Queries without a central vertex take a fifth, list-walking tier.
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <mutex>
 
 #include <cub/cub.cuh>
@@ -2582,9 +2583,28 @@ beep_status launch_general(int dend, int grid, cudaStream_t s, const PairDev *pa
     return BEEP_OK;
 }
 
+// Raises a kernel's dynamic shared memory limit on the current device, never
+// lowers it. A plan sets the limits its launches need when it is made and
+// replays them later (eagerly or from a captured CUDA graph); a plan made in
+// between for smaller domains must not leave an earlier plan's launches above
+// the limit (they would fail with an invalid argument).
+beep_status raise_smem_limit(const void *fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> limits;
+    int dev = 0;
+    BEEP_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = limits[{dev, fn}];
+    if (bytes <= cur)
+        return BEEP_OK;
+    BEEP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+    return BEEP_OK;
+}
+
 template <int D, bool ENUM> beep_status set_medium_attr(size_t smem) {
-    BEEP_CUDA_TRY(cudaFuncSetAttribute(k_medium<D, ENUM, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    BEEP_CUDA_TRY(cudaFuncSetAttribute(k_medium<D, ENUM, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BEEP_TRY(raise_smem_limit((const void *)k_medium<D, ENUM, 0>, smem));
+    BEEP_TRY(raise_smem_limit((const void *)k_medium<D, ENUM, 32>, smem));
     return BEEP_OK;
 }
 
@@ -2992,7 +3012,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         BEEP_CUDA_TRY(cudaMemsetAsync(tstart, 0, 4, s));
         const uint32_t maxD_all = tier_max[3];
         const size_t smemA = std::min<size_t>(maxD_all, kLargeSmemA) * 4;
-        BEEP_CUDA_TRY(cudaFuncSetAttribute(k_large_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemA));
+        BEEP_TRY(raise_smem_limit((const void *)k_large_rows, smemA));
         LaunchRec ms;
         ms.kind = LaunchRec::kMemset;
         ms.mptr = arena;
@@ -3088,7 +3108,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         BEEP_TRY(lp->alloc(arena, arena_words));
         const uint32_t maxD_all = rs[0].D;
         const size_t smemA = std::min<size_t>(maxD_all, kLargeSmemA) * 4;
-        BEEP_CUDA_TRY(cudaFuncSetAttribute(k_large_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemA));
+        BEEP_TRY(raise_smem_limit((const void *)k_large_rows, smemA));
         for (auto &bb : batches) {
             const size_t i0 = bb.first, i1 = bb.second;
             std::stable_sort(rs.begin() + i0, rs.begin() + i1,

@@ -110,7 +110,9 @@ def test_batch_with_hub_roots_equals_plain_loop(ctx):
     """A small slice of the batched workload whose graphs have hubs above
     degree 1,024: every large-tier kernel (walks with donation, the 4-wheel,
     the neighbourhood statistics) runs in one plan over all 15 central
-    patterns, and each count equals the same pair counted alone."""
+    patterns, and each count equals the same pair counted alone. The plain
+    counts in between plan smaller launches; the captured replay after them
+    still runs the batch's own (shared memory limits only grow)."""
     gs = [B.gen_chung_lu(1 << 14, 32.0, 2.1, 13000 + i) for i in range(3)]
     assert all(np.diff(rp).max() > 1024 for rp, _ in gs)
     graphs = [B.Graph.from_csr(ctx, rp, col) for rp, col in gs]
