@@ -3485,17 +3485,23 @@ static cudaError_t readback(LaunchPlan *lp, cudaStream_t s, bool timing) {
 static beep_status donation_result(const LaunchPlan *lp, uint64_t *donated) {
     const unsigned *ctl = reinterpret_cast<const unsigned *>(lp->h_counts + kPairWords * (size_t)lp->np + kAux);
     uint64_t d = 0;
-    bool timed_out = false;
+    std::string where;
     for (uint32_t i = 0; i < lp->ndon; ++i) {
-        d += ctl[(size_t)i * kDonWords + kDonCount];
-        timed_out |= ctl[(size_t)i * kDonWords + kDonError] != 0;
+        const unsigned *c = ctl + (size_t)i * kDonWords;
+        d += c[kDonCount];
+        if (c[kDonError] && where.empty())
+            where = "walk launch " + std::to_string(i) + " of " + std::to_string(lp->ndon) + ": slots claimed " +
+                    std::to_string(c[kDonHead]) + ", reserved " + std::to_string(c[kDonTail]) + ", pending " +
+                    std::to_string(c[kDonPending]) + ", static tasks done " + std::to_string(c[kDonStaticDone]) +
+                    ", donated done " + std::to_string(c[kDonDone]) + ", heartbeats " +
+                    std::to_string(c[kDonHeartbeat]);
     }
     if (donated)
         *donated = d;
-    if (timed_out)
+    if (!where.empty())
         return fail(BEEP_ERR_TIMEOUT, "a warp of the large tier waited for donated work longer than the wait "
                                       "timeout with no progress anywhere (beep_ctx_set_wait_timeout); the counts of "
-                                      "this run are incomplete");
+                                      "this run are incomplete (" + where + ")");
     return BEEP_OK;
 }
 
