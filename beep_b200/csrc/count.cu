@@ -1495,6 +1495,7 @@ struct Batch {
 constexpr uint32_t kRowsPerChunk = 256;
 constexpr int kLargeDfsBlocksPerSm = 8; // k_large_wheel grid: 256-thread blocks per SM
 constexpr uint32_t kDonCap = 1u << 18;   // donated tasks per walk launch (16 MiB of records)
+constexpr uint32_t kCursorBlock = 256;   // work cursors allocated at a time
 constexpr uint32_t kMaxDonLaunches = 64; // walk launches of a call with a donation queue
 // Depth slot of a root in the tier lists: its plan's depth, except the large
 // tier's 4-wheel roots, which take slot 2 (no plan has depth 2) and run on
@@ -2703,7 +2704,9 @@ struct LaunchPlan {
     uint64_t N = 0;
     // per pair (count, overflow flag), then np tuple counters, then kAux byte counters
     unsigned long long *d_counts = nullptr;
-    unsigned *d_cursors = nullptr;
+    // work cursors, one per launch that takes items from a counter: blocks
+    // of kCursorBlock, all zeroed at the start of every run
+    std::vector<unsigned *> cursor_blocks;
     uint32_t ncursors = 0;
     // pinned mirror of the (count, flag) words and the byte counters (2 np + kAux):
     // the context's buffer, or owned when captured
@@ -2819,8 +2822,6 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     lp->np = np;
     tr.mark("views");
     BEEP_TRY(lp->alloc(lp->d_counts, (kPairWords + 1) * (size_t)np + kAux));
-    lp->ncursors = 64;
-    BEEP_TRY(lp->alloc(lp->d_cursors, lp->ncursors));
     if (np == 0) {
         BEEP_TRY(ctx->host_results(lp->host_words(), &lp->h_counts));
         *out = std::move(lp);
@@ -2889,8 +2890,18 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
     st.roots_general = tier_n[4];
     st.roots = st.roots_small + st.roots_medium + st.roots_large + st.roots_general;
     tr.mark("classify");
-    uint32_t next_cursor = 0;
-    auto cursor = [&]() -> unsigned * { return lp->d_cursors + (next_cursor++ % lp->ncursors); };
+    // a fresh zeroed work counter for every launch (a shared one would make a
+    // later launch start past its first items and skip them)
+    auto cursor = [&](unsigned *&out) -> beep_status {
+        if (lp->ncursors % kCursorBlock == 0) {
+            unsigned *blk = nullptr;
+            BEEP_TRY(lp->alloc(blk, kCursorBlock));
+            lp->cursor_blocks.push_back(blk);
+        }
+        const uint32_t i = lp->ncursors++;
+        out = lp->cursor_blocks[i / kCursorBlock] + i % kCursorBlock;
+        return BEEP_OK;
+    };
     // a walk launch of the large tier: a persistent grid of resident blocks,
     // and (for k_large_dfs) the donation queue, whose ready flags are cleared
     // before the launch
@@ -3026,7 +3037,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         lr.smem = smemA;
         lr.bt = Batch{list, reinterpret_cast<const uint64_t *>(boff), cstart, tstart, nl};
         lr.mptr = arena;
-        lr.cursor = cursor();
+        BEEP_TRY(cursor(lr.cursor));
         lr.sink = &st.large_encode_ms;
         lp->recs.push_back(lr);
         if (list_cap((maxD_all + 31) / 32))
@@ -3049,7 +3060,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             ld.bt = Batch{list + first, reinterpret_cast<const uint64_t *>(boff) + first, cstart, tstart + first,
                           cnt};
             ld.mptr = arena;
-            ld.cursor = cursor();
+            BEEP_TRY(cursor(ld.cursor));
             ld.sink = &st.large_dfs_ms;
             ld.wsc = wsc;
             ld.wstride = wstride;
@@ -3167,7 +3178,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             lr.smem = smemA;
             lr.bt = Batch{d_bitem, d_boff, d_cs, d_ts, nbt};
             lr.mptr = arena;
-            lr.cursor = cursor();
+            BEEP_TRY(cursor(lr.cursor));
             lr.sink = &st.large_encode_ms;
             lp->recs.push_back(lr);
             if (list_cap((bmaxD + 31) / 32))
@@ -3190,7 +3201,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
                 ld.bt = Batch{d_bitem + groups[gi].first, d_boff + groups[gi].first, d_cs, d_ts + ts_off[gi],
                               groups[gi].second};
                 ld.mptr = arena;
-                ld.cursor = cursor();
+                BEEP_TRY(cursor(ld.cursor));
                 ld.sink = &st.large_dfs_ms;
                 ld.wsc = wsc;
                 ld.wstride = wstride;
@@ -3230,7 +3241,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             r.items = list + first;
             r.n = cnt;
             r.maxD = maxD;
-            r.cursor = cursor();
+            BEEP_TRY(cursor(r.cursor));
             r.sink = &st.medium_ms;
             r.tail_slot = 1;
             lp->recs.push_back(r);
@@ -3301,7 +3312,7 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
             r.items = list + first;
             r.tstart = tstart + first;
             r.n = cnt;
-            r.cursor = cursor();
+            BEEP_TRY(cursor(r.cursor));
             r.sink = &st.general_ms;
             lp->recs.push_back(r);
             first += cnt;
@@ -3336,7 +3347,8 @@ beep_status issue(Ctx *ctx, LaunchPlan *lp, bool timing, bool serial, bool stall
     cudaStream_t s = ctx->stream;
     const uint32_t np = lp->np;
     BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_counts, 0, ((kPairWords + 1) * (size_t)np + kAux) * 8, s));
-    BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_cursors, 0, lp->ncursors * 4, s));
+    for (unsigned *blk : lp->cursor_blocks)
+        BEEP_CUDA_TRY(cudaMemsetAsync(blk, 0, kCursorBlock * 4, s));
     if (lp->ndon) {
         BEEP_CUDA_TRY(cudaMemsetAsync(lp->d_don_ctl, 0, (size_t)lp->ndon * kDonWords * 4, s));
         if (stall_test) // one phantom donated task that no donor publishes: every wait runs out

@@ -714,12 +714,16 @@ def bench_served(args) -> dict:
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     serial = []
+    by_kind = {}  # serial seconds per (pattern, count or first-k) kind: where the GPU time goes
     for gi, nm, k in reqs:
+        t1 = time.perf_counter()
         if k:
             _, tot = B.enumerate_matches(graphs[gi], queries[nm], k)
             serial.append(tot)
         else:
             serial.append(B.count(graphs[gi], queries[nm]))
+        kind = f"{nm}/{'first-k' if k else 'count'}"
+        by_kind[kind] = by_kind.get(kind, 0.0) + time.perf_counter() - t1
     serial_s = time.perf_counter() - t0
     note(f"c5: serial run of {n_req} requests {serial_s:.1f} s")
     srv = B.Server(ctx, max_batch=args.c5_max_batch, streams=args.c5_streams)
@@ -744,7 +748,8 @@ def bench_served(args) -> dict:
                       "streams": args.c5_streams,
                       "edges_directed": int(sum(len(c) for _, c in host))},
            "matches": int(total),
-           "serial_plain": {"value": total / serial_s, "s": serial_s},
+           "serial_plain": {"value": total / serial_s, "s": serial_s,
+                            "s_by_kind": {k: round(v, 3) for k, v in sorted(by_kind.items(), key=lambda x: -x[1])}},
            "speedup_vs_serial_plain": (total / st["span_s"]) / (total / serial_s),
            "batches": st["batches"], "largest_batch": st["max_batch"], "span_s": st["span_s"],
            "offered_span_s": float(arrivals[-1]) if n_req else 0.0}
@@ -761,7 +766,7 @@ def bench_served(args) -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
