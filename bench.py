@@ -591,6 +591,21 @@ def c4_graph_specs(n_graphs, lo_scale, hi_scale, dmin, dmax, seed=13):
     return specs
 
 
+def pattern_label(edges, index) -> str:
+    """'<index>:<name>' for a query edge list: its name among the named
+    patterns when it is one of them, else its vertex and edge counts."""
+    from beep_b200 import patterns as P
+
+    n = max(max(a, b) for a, b in edges) + 1
+    und = sorted({(min(a, b), max(a, b)) for a, b in edges})
+    canon = P._canon(n, und)
+    for name, q in P.NAMED.items():
+        qn = max(max(a, b) for a, b in q) + 1
+        if qn == n and P._canon(qn, sorted({(min(a, b), max(a, b)) for a, b in q})) == canon:
+            return f"{index}:{name}"
+    return f"{index}:{n}v{len(und)}e"
+
+
 def bench_batched(args) -> dict:
     import torch
 
@@ -605,7 +620,8 @@ def bench_batched(args) -> dict:
     gen_s = time.perf_counter() - t0
     graphs = [B.Graph.from_csr(ctx, rp, col) for rp, col in host]
     note(f"c4: {len(graphs)} graphs generated in {gen_s:.1f} s, {sum(len(c) for _, c in host)} directed edges")
-    pats = [B.Query.from_edges(q) for q in P.central_patterns(4) + P.central_patterns(5)]
+    qedges = P.central_patterns(4) + P.central_patterns(5)
+    pats = [B.Query.from_edges(q) for q in qedges]
     pairs = [(gi, qi) for gi in range(len(graphs)) for qi in range(len(pats))]
 
     def plain(gi, qi):
@@ -634,7 +650,12 @@ def bench_batched(args) -> dict:
     # plain loop: one count per pair, views resident
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    plain_counts = [plain(gi, qi) for gi, qi in pairs]
+    plain_counts = []
+    by_pattern = [0.0] * len(pats)  # per-pair loop seconds per pattern: where the GPU time goes
+    for gi, qi in pairs:
+        t1 = time.perf_counter()
+        plain_counts.append(plain(gi, qi))
+        by_pattern[qi] += time.perf_counter() - t1
     plain_s = time.perf_counter() - t0
     note(f"c4: per-pair loop {plain_s:.1f} s")
     clocks = ClockSampler(0)
@@ -672,7 +693,9 @@ def bench_batched(args) -> dict:
            "overflow_pairs": [{"graph": pairs[i][0], "graph_spec": list(specs[pairs[i][0]][:2]),
                                "pattern": pairs[i][1]} for i in over],
            "plain_loop": {"value": total / plain_s, "ms": plain_s * 1e3,
-                          "what": "beep_count per pair, same pairs, views resident, host wall time"},
+                          "what": "beep_count per pair, same pairs, views resident, host wall time",
+                          "s_by_pattern": {pattern_label(qedges[qi], qi): round(by_pattern[qi], 3) for qi in
+                                           sorted(range(len(pats)), key=lambda q: -by_pattern[q])}},
            "speedup_vs_plain_loop": plain_s / host_s,
            "speedup_note": "both sides host wall time of the calls (the replay's device time is ms_per_step)",
            "plan_and_capture_ms": plan_s * 1e3, "autotuned_tiers": tuned, "generate_s": gen_s}
