@@ -106,6 +106,14 @@ __device__ __forceinline__ unsigned long long sat_add(unsigned long long a, unsi
     return (s < a || s >= kCountLimit) ? kCountLimit : s;
 }
 
+__device__ __forceinline__ unsigned long long binom2(unsigned long long x) { return x * (x - (x ? 1 : 0)) / 2; }
+
+// 128-bit product saturated to the count limit.
+__device__ __forceinline__ unsigned long long sat_mul(unsigned long long a, unsigned long long b) {
+    const unsigned __int128 p = (unsigned __int128)a * b;
+    return p >= (unsigned __int128)kCountLimit ? kCountLimit : (unsigned long long)p;
+}
+
 // cnt + C(A, L) for L <= 4, the binomial exact through a 128-bit product
 // (A < 2^32), saturating at kCountLimit.
 __device__ __forceinline__ unsigned long long add_binom(unsigned long long cnt, uint32_t A, int L) {
@@ -895,31 +903,42 @@ __device__ __forceinline__ void build_rows_flat(const ViewDev &v, int asc, const
 //   3. warp w takes the contiguous work range [w * chunk, (w + 1) * chunk),
 //      32 items a step (consecutive lanes read consecutive list entries);
 //      each lane's row advances monotonically instead of being searched per
-//      item. A list entry is looked up in the hash (about two shared loads);
-//      the A entries of a row whose list is far longer than that part of A
-//      (nA * log2(c) * 4 < c) are instead searched in the list.
-// The hash has 2^k >= 2D slots of vertex ids (all ones: empty) with the
-// domain index beside each; multiplicative hashing, linear probing.
+//      item, its row's offsets held in registers. A list entry is looked up
+//      in the hash; the A entries of a row whose list is far longer than that
+//      part of A (nA * log2(c) * 4 < c) are instead searched in the list.
+// The hash has 2^k >= 8D slots of vertex ids (all ones: empty) with the
+// domain index beside each; multiplicative hashing, linear probing. Most
+// lookups miss (a list entry outside the domain), so a filter of 8 bits per
+// slot, indexed by three more bits of the same hash, answers most of them
+// with one shared load; at load factor <= 1/8 a lookup that passes it probes
+// about one slot. (On C2, 2D slots and no filter: k_medium 1.73 ms; 8D: 1.48;
+// 8D with the filter and the row offsets in registers: 1.44.)
 // ---------------------------------------------------------------------------
 constexpr uint32_t kHashEmpty = 0xffffffffu;
 
 __host__ __device__ __forceinline__ uint32_t hash_slots(uint32_t maxD) {
     uint32_t s = 64;
-    while (s < 2 * maxD)
+    while (s < 8 * maxD)
         s <<= 1;
     return s;
 }
 
 __device__ __forceinline__ uint32_t hash_of(uint32_t w, uint32_t hshift) { return (w * 0x9E3779B1u) >> hshift; }
 
-// Fills the hash of A[0, D) (block-wide; the caller syncs before and after).
+// Fills the hash of A[0, D) and its filter (nslots / 4 words after the
+// indices) (block-wide; the caller syncs before and after).
 __device__ __forceinline__ void hash_build(const uint32_t *A, uint32_t D, uint32_t *hkeys, uint16_t *hidx,
                                            uint32_t nslots, uint32_t hshift) {
+    uint32_t *filt = hkeys + nslots + nslots / 2;
     for (uint32_t i = threadIdx.x; i < nslots; i += blockDim.x)
         hkeys[i] = kHashEmpty;
+    for (uint32_t i = threadIdx.x; i < nslots / 4; i += blockDim.x)
+        filt[i] = 0;
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < D; i += blockDim.x) {
         const uint32_t w = A[i];
+        const uint32_t fi = (w * 0x9E3779B1u) >> (hshift - 3);
+        atomicOr(&filt[fi >> 5], 1u << (fi & 31));
         uint32_t s = hash_of(w, hshift);
         while (atomicCAS(&hkeys[s], kHashEmpty, w) != kHashEmpty)
             s = (s + 1) & (nslots - 1);
@@ -927,10 +946,13 @@ __device__ __forceinline__ void hash_build(const uint32_t *A, uint32_t D, uint32
     }
 }
 
-// Domain index of w, or -1.
+// Domain index of w, or -1 (at once when w's filter bit is clear).
 __device__ __forceinline__ int hash_find(const uint32_t *hkeys, const uint16_t *hidx, uint32_t nslots,
                                          uint32_t hshift, uint32_t w) {
-    uint32_t s = hash_of(w, hshift);
+    const uint32_t h = w * 0x9E3779B1u, fi = h >> (hshift - 3);
+    if (!((hkeys[nslots + nslots / 2 + (fi >> 5)] >> (fi & 31)) & 1u))
+        return -1;
+    uint32_t s = h >> hshift;
     for (;;) {
         const uint32_t key = hkeys[s];
         if (key == w)
@@ -991,19 +1013,34 @@ __device__ __forceinline__ void build_rows_hashed(const ViewDev &v, int asc, con
     // kU items per lane per step: their list entries are loaded before any is
     // looked up, so a lane keeps kU global loads in flight
     constexpr int kU = 4;
+    // the lane's current row in registers: its end in the item space, the
+    // list offset of its items and its length word
+    uint32_t r_end = 0, r_base = 0, r_len = 0;
+    if (t_begin + lane < t_end) {
+        r_end = s_pre[r + 1];
+        r_base = s_hb[r] - s_pre[r];
+        r_len = s_len[r];
+    }
     for (uint32_t t = t_begin + lane; t < t_end; t += 32 * kU) {
-        uint32_t rr[kU], wv[kU];
+        uint32_t rr[kU], wv[kU], lr[kU];
 #pragma unroll
         for (int j = 0; j < kU; ++j) {
             const uint32_t tj = t + 32u * j;
             rr[j] = 0xffffffffu;
             wv[j] = 0;
             if (tj < t_end) {
-                while (s_pre[r + 1] <= tj)
-                    ++r;
+                if (r_end <= tj) {
+                    do
+                        ++r;
+                    while (s_pre[r + 1] <= tj);
+                    r_end = s_pre[r + 1];
+                    r_base = s_hb[r] - s_pre[r];
+                    r_len = s_len[r];
+                }
                 rr[j] = r;
-                if (!(s_len[r] & kByA))
-                    wv[j] = v.col[s_hb[r] + (tj - s_pre[r])];
+                lr[j] = r_len;
+                if (!(r_len & kByA))
+                    wv[j] = v.col[r_base + tj];
             }
         }
 #pragma unroll
@@ -1011,7 +1048,7 @@ __device__ __forceinline__ void build_rows_hashed(const ViewDev &v, int asc, con
             const uint32_t rj = rr[j];
             if (rj == 0xffffffffu)
                 continue;
-            const uint32_t len = s_len[rj];
+            const uint32_t len = lr[j];
             const uint32_t xb = asc ? max(rj + 1, rlo) : 0, xe = asc ? D : rj;
             if (len & kByA) {
                 const uint32_t k = xb + (t + 32u * j - s_pre[rj]);
@@ -1301,6 +1338,184 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
 }
 
 // ---------------------------------------------------------------------------
+// neighbourhood statistics in the medium tier (counts only). A five-vertex
+// query whose plan has a statistics form (NbForm) is counted at a root from
+// the root's rows of the whole domain, already in shared memory: d_u (popcount
+// of row u), E and, per edge (u, w), the common neighbours row(u) & row(w) --
+// the terms nbhd_task sums in the large tier, over the tasks u >= j0, into
+// plus / minus. The walk would instead enumerate every (x1, x2, x3) prefix.
+// Block-wide (block-uniform call); s_deg: D words, s_misc: 2 words.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void nbhd_term(int form, unsigned long long du, unsigned long long dw, uint32_t c_all,
+                                          uint32_t c_above, unsigned long long rest, unsigned long long &plus,
+                                          unsigned long long &minus, unsigned long long &tri) {
+    switch (form) {
+    case kNbTriIso: // triangles (u < w < x) once, times the isolated vertex's choices
+        plus = sat_add(plus, sat_mul(c_above, rest));
+        break;
+    case kNbPath4: // paths x - u - w - y, minus the closed ones (x = y): 3T
+        plus = sat_add(plus, (du - 1) * (dw - 1));
+        minus = sat_add(minus, c_all);
+        break;
+    case kNbPaw: // triangles (u, w, x) with x after w: each once
+        tri += c_above;
+        break;
+    case kNbDiamond: // C(common neighbours, 2) of the edge (u, w)
+        plus = sat_add(plus, binom2(c_all));
+        break;
+    default:
+        break;
+    }
+}
+
+// Degrees of rows[0, D) into s_deg and their sum into s_misc[0]; a warp per
+// row (rw words of 32 bits, at most 32), or a thread per row (rw > 32 words
+// never occur here: the thread sub-tier's rows are 8 words).
+__device__ __forceinline__ void nbhd_degrees(const uint32_t *rows, uint32_t rw, uint32_t D, uint32_t *s_deg,
+                                             uint32_t *s_misc) {
+    const int lane = threadIdx.x & 31;
+    uint32_t part = 0;
+    for (uint32_t u = threadIdx.x >> 5; u < D; u += blockDim.x >> 5) {
+        uint32_t d = (uint32_t)lane < rw ? (uint32_t)__popc(rows[(size_t)u * rw + lane]) : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            d += __shfl_xor_sync(kFull, d, o);
+        if (lane == 0) {
+            s_deg[u] = d;
+            part += d;
+        }
+    }
+    if (lane == 0 && part)
+        atomicAdd(&s_misc[0], part);
+}
+
+// Thread sub-tier: rows of NW 64-bit words, a thread per task u.
+template <int NW>
+__device__ __forceinline__ void nbhd_medium_thread(int form, const uint64_t *r64, uint32_t D, uint32_t j0,
+                                                   uint32_t *s_deg, uint32_t *s_misc, unsigned long long &plus,
+                                                   unsigned long long &minus) {
+    if (threadIdx.x == 0) {
+        s_misc[0] = 0;
+        s_misc[1] = j0;
+    }
+    __syncthreads();
+    nbhd_degrees(reinterpret_cast<const uint32_t *>(r64), 2 * NW, D, s_deg, s_misc);
+    __syncthreads();
+    const unsigned long long E = s_misc[0] / 2, rest = D >= 3 ? D - 3 : 0;
+    if (form == kNbTwoEdges && threadIdx.x == 0)
+        plus = sat_add(plus, binom2(E)); // C(E, 2): E < 2^15 here
+    for (;;) {
+        const uint32_t u = atomicAdd(&s_misc[1], 1u);
+        if (u >= D)
+            break;
+        const unsigned long long du = s_deg[u];
+        if (form == kNbWedgeIso) {
+            plus = sat_add(plus, binom2(du) * rest);
+            continue;
+        }
+        if (form == kNbTwoEdges) {
+            minus = sat_add(minus, binom2(du));
+            continue;
+        }
+        uint64_t ru[NW];
+#pragma unroll
+        for (int i = 0; i < NW; ++i)
+            ru[i] = r64[(size_t)u * NW + i];
+        const bool all_w = form == kNbPaw; // else the edges (u, w) with w after u
+        const uint32_t ui = u >> 6;
+        unsigned long long tri = 0;
+#pragma unroll
+        for (int i = 0; i < NW; ++i) {
+            uint64_t bits = ru[i];
+            if (!all_w)
+                bits = (uint32_t)i < ui ? 0ull : ((uint32_t)i == ui ? (bits & ~((2ull << (u & 63)) - 1ull)) : bits);
+            while (bits) {
+                const uint32_t w = (uint32_t)i * 64 + (uint32_t)(__ffsll((long long)bits) - 1);
+                bits &= bits - 1;
+                const uint64_t *rw = r64 + (size_t)w * NW;
+                const uint32_t wi = w >> 6;
+                const uint64_t wm = ~((2ull << (w & 63)) - 1ull); // bits of word wi above w
+                uint32_t c_all = 0, c_above = 0;
+#pragma unroll
+                for (int k = 0; k < NW; ++k) {
+                    const uint64_t x = ru[k] & rw[k];
+                    c_all += (uint32_t)__popcll(x);
+                    c_above += (uint32_t)__popcll((uint32_t)k < wi ? 0ull : ((uint32_t)k == wi ? (x & wm) : x));
+                }
+                nbhd_term(form, du, s_deg[w], c_all, c_above, rest, plus, minus, tri);
+            }
+        }
+        if (form == kNbPaw && du >= 2)
+            plus = sat_add(plus, sat_mul(tri, du - 2));
+    }
+}
+
+// Warp sub-tier: rows of W <= 32 words, a warp per task u (lane k holds word
+// k of row u; each edge's common neighbours are one warp sum).
+__device__ __forceinline__ void nbhd_medium_warp(int form, const uint32_t *rows, uint32_t W, uint32_t D,
+                                                 uint32_t j0, uint32_t *s_deg, uint32_t *s_misc,
+                                                 unsigned long long &plus, unsigned long long &minus) {
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        s_misc[0] = 0;
+        s_misc[1] = j0;
+    }
+    __syncthreads();
+    nbhd_degrees(rows, W, D, s_deg, s_misc);
+    __syncthreads();
+    const unsigned long long E = s_misc[0] / 2, rest = D >= 3 ? D - 3 : 0;
+    if (form == kNbTwoEdges && threadIdx.x == 0)
+        plus = sat_add(plus, binom2(E)); // C(E, 2): E < 2^19 here
+    for (;;) {
+        uint32_t u = 0;
+        if (lane == 0)
+            u = atomicAdd(&s_misc[1], 1u);
+        u = __shfl_sync(kFull, u, 0);
+        if (u >= D)
+            break;
+        const unsigned long long du = s_deg[u];
+        if (form == kNbWedgeIso || form == kNbTwoEdges) {
+            if (lane == 0) {
+                if (form == kNbWedgeIso)
+                    plus = sat_add(plus, binom2(du) * rest);
+                else
+                    minus = sat_add(minus, binom2(du));
+            }
+            continue;
+        }
+        const uint32_t ru = (uint32_t)lane < W ? rows[(size_t)u * W + lane] : 0u;
+        const uint32_t uw = u >> 5;
+        uint32_t bits = ru;
+        if (form != kNbPaw)
+            bits = (uint32_t)lane < uw ? 0u : ((uint32_t)lane == uw ? (bits & ~((2u << (u & 31)) - 1u)) : bits);
+        unsigned long long tri = 0;
+        unsigned bal = __ballot_sync(kFull, bits != 0);
+        while (bal) {
+            const int L = __ffs(bal) - 1;
+            const uint32_t wb = __shfl_sync(kFull, bits, L);
+            const uint32_t w = (uint32_t)L * 32 + (uint32_t)(__ffs(wb) - 1);
+            if (lane == L)
+                bits &= bits - 1;
+            bal = __ballot_sync(kFull, bits != 0);
+            const uint32_t x = (uint32_t)lane < W ? (ru & rows[(size_t)w * W + lane]) : 0u;
+            const uint32_t wi = w >> 5;
+            uint32_t c_all = (uint32_t)__popc(x);
+            uint32_t c_above = (uint32_t)__popc((uint32_t)lane < wi ? 0u
+                                                                     : ((uint32_t)lane == wi ? (x & ~((2u << (w & 31)) - 1u)) : x));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                c_all += __shfl_xor_sync(kFull, c_all, o);
+                c_above += __shfl_xor_sync(kFull, c_above, o);
+            }
+            if (lane == 0)
+                nbhd_term(form, du, s_deg[w], c_all, c_above, rest, plus, minus, tri);
+        }
+        if (form == kNbPaw && lane == 0 && du >= 2)
+            plus = sat_add(plus, sat_mul(tri, du - 2));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // medium tier: block per root, bitmap in shared memory
 // ---------------------------------------------------------------------------
 // G lanes per level-1 vertex (32: domains of up to 1024 vertices, rows of up
@@ -1324,13 +1539,15 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
     uint32_t *s_pre = sm + 2 * pad;
     uint32_t *s_len = sm + 3 * pad;
     uint32_t *hkeys = sm + 4 * pad;                                 // domain hash: vertex ids ...
-    uint16_t *hidx = reinterpret_cast<uint16_t *>(hkeys + nslots); // ... and their domain indices
-    uint32_t *rows = hkeys + nslots + nslots / 2;
+    uint16_t *hidx = reinterpret_cast<uint16_t *>(hkeys + nslots); // ... their domain indices, the filter
+    uint32_t *rows = hkeys + nslots + nslots / 2 + nslots / 4;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
     EnumCtx ec;
     unsigned long long cnt = 0;
     bool wheel = false; // the 4-wheel's closed form (counts)
+    int nbform = kNbNone; // a neighbourhood-statistics form (counts)
+    unsigned long long nb_plus = 0, nb_minus = 0;
     for (;;) {
         if (threadIdx.x == 0)
             s_ri = atomicAdd(cursor, 1u);
@@ -1342,14 +1559,20 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
         const uint32_t p = item_pair(it), r = item_root(it);
         if (p != cur) { // block-uniform
             cnt = warp_sum(cnt);
-            if (lane == 0)
+            nb_plus = warp_sum(nb_plus);
+            nb_minus = warp_sum(nb_minus);
+            if (lane == 0) {
                 flush_count(pr.count, cnt);
-            cnt = 0;
+                flush_count(pr.count + 2, nb_plus);
+                flush_count(pr.count + 4, nb_minus);
+            }
+            cnt = nb_plus = nb_minus = 0;
             cur = p;
             load_pair(pairs, p, pr);
             if constexpr (ENUM)
                 make_ec(ec, pairs[p].en, pairs[p].pl, pr.v);
             wheel = DEND == 5 && !ENUM && pairs[p].pl.wheel4;
+            nbform = (DEND == 5 && !ENUM) ? (int)pairs[p].pl.nbhd : (int)kNbNone;
         }
         uint32_t beg, D, j0;
         pair_domain(pr, r, beg, D, j0);
@@ -1390,7 +1613,19 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
             ec.A = A;
             ec.root = r;
         }
-        if constexpr (G == 0) {
+        bool stats_done = false; // counted by the neighbourhood statistics
+        if constexpr (DEND == 5 && !ENUM) {
+            if (nbform) { // block-uniform; rows of the whole domain
+                if constexpr (G == 0)
+                    nbhd_medium_thread<kThreadNW>(nbform, reinterpret_cast<const uint64_t *>(rows), D, j0, s_hb,
+                                                  s_len, nb_plus, nb_minus);
+                else
+                    nbhd_medium_warp(nbform, rows, W, D, j0, s_hb, s_len, nb_plus, nb_minus);
+                stats_done = true;
+            }
+        }
+        if (stats_done) {
+        } else if constexpr (G == 0) {
             const uint64_t *r64 = reinterpret_cast<const uint64_t *>(rows);
             if (wheel) { // block-uniform; rows of the whole domain
                 for (;;) {
@@ -1475,8 +1710,13 @@ __global__ void __launch_bounds__(G == 0 ? 256 : 1024, G == 0 ? (DEND <= 5 ? 4 :
         __syncthreads();
     }
     cnt = warp_sum(cnt);
-    if (lane == 0)
+    nb_plus = warp_sum(nb_plus);
+    nb_minus = warp_sum(nb_minus);
+    if (lane == 0) {
         flush_count(pr.count, cnt);
+        flush_count(pr.count + 2, nb_plus);
+        flush_count(pr.count + 4, nb_minus);
+    }
     if (threadIdx.x == 0)
         record_exit(exit_t);
 }
@@ -2038,14 +2278,6 @@ __device__ __forceinline__ uint32_t common_count(const uint32_t *ra, const uint3
         s += (uint32_t)__popc(w);
     }
     return s;
-}
-
-__device__ __forceinline__ unsigned long long binom2(unsigned long long x) { return x * (x - (x ? 1 : 0)) / 2; }
-
-// 128-bit product saturated to the count limit.
-__device__ __forceinline__ unsigned long long sat_mul(unsigned long long a, unsigned long long b) {
-    const unsigned __int128 p = (unsigned __int128)a * b;
-    return p >= (unsigned __int128)kCountLimit ? kCountLimit : (unsigned long long)p;
 }
 
 // Task (root, u): u's terms of the root's form, into plus / minus (lane
@@ -3221,8 +3453,9 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         // 32-bit words per row: 8 (4 x 64 bits) in the thread-mode sub-tier
         const uint32_t W = sub == 0 ? 2 * kThreadNW : (maxD + 31) / 32;
         const size_t pad = (maxD + 4) & ~3u;
-        const size_t nslots = hash_slots(maxD); // the domain hash: nslots ids and nslots 16-bit indices
-        const size_t smem = (4 * pad + nslots + nslots / 2 + (size_t)maxD * W) * 4;
+        // the domain hash: nslots ids, nslots 16-bit indices and the filter
+        const size_t nslots = hash_slots(maxD);
+        const size_t smem = (4 * pad + nslots + nslots / 2 + nslots / 4 + (size_t)maxD * W) * 4;
         const int block = sub == 0 ? 256 : 1024;
         const int per_sm = std::max(1, (int)std::min<size_t>(2048 / block, (200 * 1024) / (smem + 1024)));
         uint32_t first = 0;

@@ -111,3 +111,34 @@ def test_forms_with_word_lists_match_the_walk(ctx):
     assert all(c > 0 for c in got)
     b.close()
     g.close()
+
+
+@pytest.mark.parametrize("graph", ["hubs_thread", "hubs_warp", "roots_thread", "roots_warp"])
+def test_forms_in_the_medium_tier(ctx, graph):
+    """The same forms counted by the medium tier from its shared-memory rows:
+    domains of 65-256 vertices (thread sub-tier, rows of 4 x 64 bits) and of
+    257-1,024 (warp sub-tier). Each count equals the oracle's and the walk's,
+    and the medium tier took roots."""
+    if graph == "hubs_thread":
+        rp, col = hubs(200, 0.06, 7, n_hubs=3)
+        forms = [6, 7, 9, 10]
+    elif graph == "hubs_warp":
+        rp, col = hubs(700, 0.02, 8, n_hubs=2)
+        forms = [6, 7, 9, 10]
+    elif graph == "roots_thread":
+        rp, col = roots_over_hubs(300, 200, 0.12, 9)
+        forms = [11, 13]
+    else:
+        rp, col = roots_over_hubs(120, 600, 0.04, 10)
+        forms = [11, 13]
+    g = B.Graph.from_csr(ctx, rp, col)
+    pats = P.central_patterns(4) + P.central_patterns(5)
+    for i in forms:
+        for seed in (0, 2):
+            q = relabel(pats[i], seed)
+            exp = O.count(rp, col, q, apply_root_cap=False)["count"]
+            c, st = B.count(g, q, B.SGM, B.OPT_TIMING, stats=True)
+            assert c == exp, (graph, i, seed)
+            assert st["roots_medium"] >= 1 and st["roots_large"] == 0, (graph, i, st["roots_medium"])
+            assert B.count(g, q, B.SGM, B.OPT_NO_NBHD) == exp, (graph, i, seed)
+    g.close()
