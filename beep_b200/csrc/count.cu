@@ -732,9 +732,12 @@ __device__ __forceinline__ void make_ec(EnumCtx &ec, const EnumDev &en, const De
 //      by binary search on the prefix, loads the element (consecutive t read
 //      consecutive addresses) and binary-searches it in A, setting both bits
 //      of every edge found.
-// Used by a block on a chunk of rows (large tier, whose domains are too large
-// for a shared-memory hash); the small and medium tiers look list entries up
-// in a hash of the domain instead (build_rows_hashed, build_rows_hashed_group).
+// Used by a warp group (small tier: a binary search over at most 64 entries;
+// a per-group hash measured slower, 0.80 -> 1.10 ms on C2, its set-up costing
+// more than the searches it saves on such small domains) or a block on a
+// chunk of rows (large tier, whose domains are too large for a shared-memory
+// hash); the medium tier looks list entries up in a hash of the domain
+// (build_rows_hashed).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t upper_bound_g(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi,
                                                   uint32_t key) {
@@ -774,9 +777,6 @@ __device__ __forceinline__ void group_excl_scan(uint32_t *buf, uint32_t R, int g
 __device__ __forceinline__ void warp_excl_scan(uint32_t *buf, uint32_t R, int lane) {
     group_excl_scan<32>(buf, R, lane, kFull);
 }
-
-// floor(log2(x)) for x >= 1, at compile time
-__host__ __device__ constexpr uint32_t ilog2_const(uint32_t x) { return x <= 1 ? 0u : 1u + ilog2_const(x >> 1); }
 
 // G = 0: the whole block; else a group of G lanes of one warp.
 template <int G> __device__ __forceinline__ void group_sync(unsigned gmask) {
@@ -1068,124 +1068,6 @@ __device__ __forceinline__ void build_rows_hashed(const ViewDev &v, int asc, con
     }
 }
 
-// The same hash and row builder for a group of G lanes of one warp (small
-// tier, domains of at most 64 vertices): the group's own hash of A, its rows'
-// items taken glane, glane + G, ... (consecutive lanes read consecutive list
-// entries, each lane's row only moves forward, its offsets in registers).
-// The binary search of every item in A (6 dependent shared loads at D = 64)
-// becomes one filter load for most items.
-template <int G>
-__device__ __forceinline__ void hash_build_group(const uint32_t *A, uint32_t D, uint32_t *hkeys, uint16_t *hidx,
-                                                 uint32_t nslots, uint32_t hshift, uint32_t glane, unsigned gmask) {
-    uint32_t *filt = hkeys + nslots + nslots / 2;
-    for (uint32_t i = glane; i < nslots; i += G)
-        hkeys[i] = kHashEmpty;
-    for (uint32_t i = glane; i < nslots / 4; i += G)
-        filt[i] = 0;
-    group_sync<G>(gmask);
-    for (uint32_t i = glane; i < D; i += G) {
-        const uint32_t w = A[i];
-        const uint32_t fi = (w * 0x9E3779B1u) >> (hshift - 3);
-        atomicOr(&filt[fi >> 5], 1u << (fi & 31));
-        uint32_t sl = hash_of(w, hshift);
-        while (atomicCAS(&hkeys[sl], kHashEmpty, w) != kHashEmpty)
-            sl = (sl + 1) & (nslots - 1);
-        hidx[sl] = (uint16_t)i;
-    }
-    group_sync<G>(gmask);
-}
-
-template <int G, typename SetFn>
-__device__ __forceinline__ void build_rows_hashed_group(const ViewDev &v, int asc, const uint32_t *A, uint32_t D,
-                                                        uint32_t rlo, uint32_t *s_hb, uint32_t *s_pre,
-                                                        uint32_t *s_len, const uint32_t *hkeys, const uint16_t *hidx,
-                                                        uint32_t nslots, uint32_t hshift, uint32_t glane,
-                                                        unsigned gmask, SetFn set) {
-    constexpr uint32_t kByA = 0x80000000u;
-    for (uint32_t r = glane; r < D; r += G) {
-        uint32_t hb, he, xb, xe, work = 0, len = 0;
-        hd_range(v, asc, A[r], r, D, hb, he, xb, xe);
-        if (asc)
-            xb = max(xb, rlo);
-        else if (r < rlo)
-            xe = 0;
-        if (xb < xe && hb < he) {
-            const uint32_t c = he - hb, nA = xe - xb;
-            len = c;
-            work = c;
-            if (c < kByA && (uint64_t)nA * search_steps(c) * 4 < (uint64_t)c) {
-                len = c | kByA;
-                work = nA;
-            }
-        }
-        s_hb[r] = hb;
-        s_len[r] = len;
-        s_pre[r] = work;
-    }
-    group_sync<G>(gmask);
-    group_excl_scan<G>(s_pre, D, (int)glane, gmask);
-    group_sync<G>(gmask);
-    const uint32_t T = s_pre[D];
-    uint32_t r = 0, r_end = 0, r_base = 0, r_len = 0;
-    if (glane < T) { // the row of this lane's first item: last r with s_pre[r] <= glane
-        uint32_t lo = 0, hi = D;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_pre[mid] <= glane)
-                lo = mid;
-            else
-                hi = mid;
-        }
-        r = lo;
-        r_end = s_pre[r + 1];
-        r_base = s_hb[r] - s_pre[r];
-        r_len = s_len[r];
-    }
-    constexpr int kU = 4;
-    for (uint32_t t = glane; t < T; t += G * kU) {
-        uint32_t rr[kU], wv[kU], lr[kU];
-#pragma unroll
-        for (int j = 0; j < kU; ++j) {
-            const uint32_t tj = t + (uint32_t)G * j;
-            rr[j] = 0xffffffffu;
-            wv[j] = 0;
-            lr[j] = 0;
-            if (tj < T) {
-                if (r_end <= tj) {
-                    do
-                        ++r;
-                    while (s_pre[r + 1] <= tj);
-                    r_end = s_pre[r + 1];
-                    r_base = s_hb[r] - s_pre[r];
-                    r_len = s_len[r];
-                }
-                rr[j] = r;
-                lr[j] = r_len;
-                if (!(r_len & kByA))
-                    wv[j] = v.col[r_base + tj];
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < kU; ++j) {
-            const uint32_t rj = rr[j];
-            if (rj == 0xffffffffu)
-                continue;
-            const uint32_t len = lr[j];
-            const uint32_t xb = asc ? max(rj + 1, rlo) : 0, xe = asc ? D : rj;
-            if (len & kByA) {
-                const uint32_t k = xb + (t + (uint32_t)G * j - s_pre[rj]);
-                const uint32_t hb = s_hb[rj];
-                if (contains_g(v.col, hb, hb + (len & ~kByA), A[k]))
-                    set(rj, k);
-            } else {
-                const int k = hash_find(hkeys, hidx, nslots, hshift, wv[j]);
-                if (k >= (int)xb && k < (int)xe)
-                    set(rj, (uint32_t)k);
-            }
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
 // work items. A pair is one (graph view, compiled query); an item is one root
 // of one pair, packed as (pair << 32) | root. One launch per tier serves the
@@ -1361,12 +1243,6 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
                                                            const uint64_t *__restrict__ items, uint32_t nitems,
                                                            unsigned long long *exit_t) {
     constexpr int NG = kSmallWarps * 32 / G; // groups per block
-    // each group's domain hash: >= 4 MAXD slots (at least 64), their 16-bit
-    // indices and the filter
-    constexpr uint32_t kSlots = (4 * MAXD < 64) ? 64u : (uint32_t)(4 * MAXD);
-    static_assert((kSlots & (kSlots - 1)) == 0, "hash slots: a power of two");
-    constexpr uint32_t kHashShift = 32u - ilog2_const(kSlots);
-    __shared__ uint32_t s_hash[NG][kSlots + kSlots / 2 + kSlots / 4];
     __shared__ uint64_t s_rows[NG][MAXD];
     __shared__ uint32_t s_A[NG][MAXD];
     __shared__ uint32_t s_hb[NG][MAXD];
@@ -1410,18 +1286,14 @@ __global__ void __launch_bounds__(kSmallWarps * 32, DEND <= 4 ? 5 : 1) k_small(c
             rows[i] = 0;
         }
         __syncwarp(gmask);
-        if (rlo < D) { // group-uniform
-            uint32_t *hk = s_hash[gid];
-            uint16_t *hi = reinterpret_cast<uint16_t *>(hk + kSlots);
-            hash_build_group<G>(A, D, hk, hi, kSlots, kHashShift, (uint32_t)glane, gmask);
-            build_rows_hashed_group<G>(pr.v, pr.asc, A, D, rlo, s_hb[gid], s_pre[gid], s_len[gid], hk, hi, kSlots,
-                                       kHashShift, (uint32_t)glane, gmask, [&](uint32_t i, uint32_t k) {
-                                           if (i >= rlo)
-                                               atomicOr((unsigned long long *)&rows[i - rlo], 1ull << k);
-                                           if (k >= rlo)
-                                               atomicOr((unsigned long long *)&rows[k - rlo], 1ull << i);
-                                       });
-        }
+        if (rlo < D)
+            build_rows_flat<G>(pr.v, pr.asc, A, D, rlo, 0, D, s_hb[gid], s_pre[gid], s_len[gid], (uint32_t)glane,
+                               (uint32_t)G, gmask, [&](uint32_t i, uint32_t k) {
+                                   if (i >= rlo)
+                                       atomicOr((unsigned long long *)&rows[i - rlo], 1ull << k);
+                                   if (k >= rlo)
+                                       atomicOr((unsigned long long *)&rows[k - rlo], 1ull << i);
+                               });
         __syncwarp(gmask);
         if constexpr (ENUM) {
             ec.A = A;
