@@ -445,6 +445,45 @@ def count(graph: Graph, query, mode: int = SGM, options: int = 0, ctx: Context |
     return (int(st.count), st.as_dict()) if stats else int(st.count)
 
 
+_TUNE_KEYS = ("tiny_max", "small_max", "med_a_max", "med_max", "donate_min_iters")
+
+
+def tune_cache_get(path: str, key: str) -> dict | None:
+    """The tier limits stored under key in the JSON file at path, or None
+    (no file, no such key, or an entry without every limit)."""
+    import json
+
+    try:
+        with open(path) as f:
+            entry = json.load(f).get(key)
+    except (OSError, ValueError, AttributeError):
+        return None
+    if not isinstance(entry, dict) or any(k not in entry for k in _TUNE_KEYS):
+        return None
+    return {k: int(entry[k]) for k in _TUNE_KEYS} | ({"count_ms": float(entry["count_ms"])}
+                                                     if "count_ms" in entry else {})
+
+
+def tune_cache_put(path: str, key: str, tiers: dict) -> None:
+    """Store the tier limits under key in the JSON file at path (other keys
+    kept; written to a temporary file and renamed into place)."""
+    import json
+
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        if not isinstance(data, dict):
+            data = {}
+    except (OSError, ValueError):
+        data = {}
+    data[key] = {k: int(tiers[k]) for k in _TUNE_KEYS} | ({"count_ms": float(tiers["count_ms"])}
+                                                          if "count_ms" in tiers else {})
+    tmp = f"{path}.tmp{os.getpid()}"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
 class Batch:
     """Many (graph, query, mode) pairs counted by one set of launches,
     captured into a CUDA graph on the first run and replayed afterwards."""
@@ -478,13 +517,25 @@ class Batch:
 
     TIER_KEYS = ("tiny_max", "small_max", "med_a_max", "med_max", "donate_min_iters")
 
-    def autotune(self, options: int = 0) -> dict:
-        """Pick the tier limits by measurement (beep_batch_autotune); returns
-        them with the best counting time in ms."""
+    def autotune(self, options: int = 0, cache: str | None = None, key: str | None = None) -> dict:
+        """Pick the tier limits (bitmap word width and lanes per root by
+        domain size, and the large tier's donation threshold) by measurement
+        (beep_batch_autotune); returns them with the best counting time in
+        ms. With cache (a JSON file) and key (a name for this workload), a
+        choice stored there under key is applied without measuring, and a new
+        one is stored under key, so a deployment tunes once per workload."""
+        if cache is not None and key is not None:
+            got = tune_cache_get(cache, key)
+            if got is not None:
+                self.set_tiers(got)
+                return {**got, "cached": True}
         cfg = (ctypes.c_uint32 * 5)()
         ms = ctypes.c_double()
         _check(lib().beep_batch_autotune(self._h, int(options), ctypes.byref(cfg), ctypes.byref(ms)))
-        return {**dict(zip(self.TIER_KEYS, list(cfg))), "count_ms": ms.value}
+        out = {**dict(zip(self.TIER_KEYS, list(cfg))), "count_ms": ms.value}
+        if cache is not None and key is not None:
+            tune_cache_put(cache, key, out)
+        return out
 
     def set_tiers(self, tiers: dict) -> None:
         vals = [int(tiers[k]) for k in self.TIER_KEYS[:4]] + [int(tiers.get("donate_min_iters", 2))]

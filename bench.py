@@ -642,7 +642,10 @@ def bench_batched(args) -> dict:
     tuned = None
     if args.c4_autotune:
         t0 = time.perf_counter()
-        tuned = batch.autotune()  # tier limits and donation threshold by measurement, before the timed replays
+        # tier limits and donation threshold by measurement (or from the tuning
+        # cache file), before the timed replays
+        tuned = batch.autotune(cache=args.c4_tune_cache,
+                               key=f"c4:{args.c4_graphs}:{args.c4_max_scale}:{args.c4_max_degree}")
         tuned["seconds"] = time.perf_counter() - t0
         note(f"c4: autotune {tuned['seconds']:.1f} s")
     t0 = time.perf_counter()
@@ -812,6 +815,8 @@ def main():
                     help="batched: pick the tier limits and donation threshold by measurement before the replays")
     ap.add_argument("--c4-no-autotune", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--c4-steps", type=int, default=2)
+    ap.add_argument("--c4-tune-cache", default=None,
+                    help="JSON file of autotuned tier limits per batched workload (read if present, else written)")
     ap.add_argument("--c5-graphs", type=int, default=32)
     ap.add_argument("--c5-max-log10-edges", type=float, default=7.0)
     ap.add_argument("--c5-rate", type=float, default=2000.0)

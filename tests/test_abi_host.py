@@ -165,3 +165,24 @@ def test_cli_help(built):
     r = subprocess.run([os.path.join(ROOT, "beep_b200", "beep"), "-m", "tc", "-g", "x", "-t", "y"],
                        capture_output=True, text=True)
     assert r.returncode != 0 and "Unrecognized" in r.stderr
+
+
+def test_tune_cache_round_trip(tmp_path):
+    """The autotuner's choice persisted per workload key in a JSON file: a
+    stored entry reads back exactly, other keys are kept, and a missing file,
+    key or limit reads as nothing."""
+    import beep_b200 as B
+
+    path = str(tmp_path / "tiers.json")
+    assert B.tune_cache_get(path, "c4") is None
+    t1 = {"tiny_max": 8, "small_max": 64, "med_a_max": 256, "med_max": 1024, "donate_min_iters": 2,
+          "count_ms": 12.5}
+    t2 = {"tiny_max": 16, "small_max": 32, "med_a_max": 128, "med_max": 512, "donate_min_iters": 0}
+    B.tune_cache_put(path, "c4", t1)
+    B.tune_cache_put(path, "other", t2)
+    assert B.tune_cache_get(path, "c4") == t1
+    assert B.tune_cache_get(path, "other") == t2
+    assert B.tune_cache_get(path, "missing") is None
+    with open(path, "w") as f:
+        f.write('{"c4": {"tiny_max": 8}}')
+    assert B.tune_cache_get(path, "c4") is None
