@@ -1908,8 +1908,8 @@ __global__ void __launch_bounds__(256) k_large_lists(const PairDev *__restrict__
 // list tl (W words each), and la (W words) for x1's non-zero words when its
 // row has no list. Rows are those of the whole domain (rlo = 0).
 __device__ __forceinline__ void wheel4_task(const uint32_t *__restrict__ bm, const RowLists &rl, uint32_t W,
-                                            uint32_t a, uint32_t *U, uint32_t *tl, uint32_t *la, int lane,
-                                            unsigned long long &cnt) {
+                                            uint32_t a, uint32_t *U, uint32_t *U2, uint32_t *tl, uint32_t *la,
+                                            int lane, unsigned long long &cnt) {
     const unsigned lt = (1u << lane) - 1u;
     const uint32_t *ra = bm + (size_t)a * W;
     const uint32_t aw = a >> 5;
@@ -1932,7 +1932,10 @@ __device__ __forceinline__ void wheel4_task(const uint32_t *__restrict__ bm, con
         __syncwarp();
     }
     // U = OR over b in row(a), b > a, of row(b)'s bits above a; tl lists U's
-    // non-zero words
+    // non-zero words. U2 keeps the bits OR-ed in at least twice: an x3 reached
+    // from one b only has c = |row(a) & row(x3) above a| = 1 and C(1, 2) = 0,
+    // so only U2's x3 need the pair phase (c counts exactly the b whose row
+    // holds x3).
     uint32_t nt = 0;
     auto or_word = [&](const uint32_t *rb, uint32_t k) {
         uint32_t v = 0;
@@ -1946,6 +1949,8 @@ __device__ __forceinline__ void wheel4_task(const uint32_t *__restrict__ bm, con
             const uint32_t old = U[k];
             fresh = old == 0;
             U[k] = old | v;
+            if (old & v)
+                U2[k] |= old & v;
         }
         const unsigned fb = __ballot_sync(kFull, fresh);
         if (fresh)
@@ -1987,8 +1992,9 @@ __device__ __forceinline__ void wheel4_task(const uint32_t *__restrict__ bm, con
             uint32_t u = 0, k = 0;
             if (t0 + (uint32_t)lane < nt) {
                 k = tl[t0 + lane];
-                u = U[k];
+                u = U2[k];
                 U[k] = 0;
+                U2[k] = 0;
             }
             for (;;) {
                 uint32_t c = 0xffffffffu;
@@ -2035,8 +2041,9 @@ __device__ __forceinline__ void wheel4_task(const uint32_t *__restrict__ bm, con
         uint32_t u = 0, k = 0;
         if (t0 + (uint32_t)lane < nt) {
             k = tl[t0 + lane];
-            u = U[k];
+            u = U2[k];
             U[k] = 0;
+            U2[k] = 0;
         }
         while (u) {
             const uint32_t c = (k << 5) + (uint32_t)(__ffs(u) - 1);
@@ -2245,9 +2252,10 @@ __global__ void __launch_bounds__(256) k_large_wheel(const PairDev *__restrict__
     const int lane = threadIdx.x & 31;
     const uint32_t base0 = bt.tstart[0];
     const uint32_t total = bt.tstart[bt.nb] - base0;
-    // three regions of Wm >= every root's W words at fixed places: U (zero
-    // on entry and on exit), U's word list, x1's word list
-    const uint32_t Wm = wstride / 3;
+    // four regions of Wm >= every root's W words at fixed places: U (zero on
+    // entry and on exit), U's word list, x1's word list, U2 (zero on entry
+    // and on exit)
+    const uint32_t Wm = wstride / 4;
     uint32_t *ws = wsc + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * wstride;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
@@ -2279,7 +2287,8 @@ __global__ void __launch_bounds__(256) k_large_wheel(const PairDev *__restrict__
         rl.cap = list_cap(W);
         rl.nzc = rows + (size_t)D * W;
         rl.nzl = rl.nzc + D;
-        wheel4_task(rows, rl, W, j0 + (t - bt.tstart[b]), ws, ws + Wm, ws + 2 * (size_t)Wm, lane, cnt);
+        wheel4_task(rows, rl, W, j0 + (t - bt.tstart[b]), ws, ws + 3 * (size_t)Wm, ws + Wm, ws + 2 * (size_t)Wm, lane,
+                    cnt);
     }
     cnt = warp_sum(cnt);
     if (lane == 0)
@@ -2457,9 +2466,10 @@ __global__ void __launch_bounds__(256) k_large_nbhd(const PairDev *__restrict__ 
     const uint32_t base0 = bt.tstart[0];
     const uint32_t total = bt.tstart[bt.nb] - base0;
     // the warp's scratch is shared with k_large_wheel, which needs its first
-    // wstride / 3 words (U, for roots of any width) zero on entry: this
-    // kernel writes only the third region, words [2 Wm, 3 Wm)
-    const uint32_t Wm = wstride / 3;
+    // and fourth regions of wstride / 4 words (U and U2, for roots of any
+    // width) zero on entry: this kernel writes only the third region, words
+    // [2 Wm, 3 Wm)
+    const uint32_t Wm = wstride / 4;
     uint32_t *ws = wsc + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * wstride;
     PairRegs pr;
     uint32_t cur = 0xffffffffu;
@@ -3286,13 +3296,13 @@ beep_status plan_pairs(Ctx *ctx, const std::vector<PairSpec> &specs, uint32_t op
         BEEP_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
         arena_cap = std::max<size_t>((size_t)256 << 20, std::min<size_t>((size_t)48 << 30, free_b / 2));
     }
-    // scratch of the large tier's 4-wheel tasks: U, its word list and x1's
-    // words (W words each) for every warp of the DFS grid, zero on entry
+    // scratch of the large tier's 4-wheel tasks: U, its word list, x1's words
+    // and U2 (W words each) for every warp of the DFS grid, zero on entry
     uint32_t *wsc = nullptr;
     uint32_t wstride = 0;
     {
         if (tier_depth[3 * kSlots + kWheelSlot] > 0 || tier_depth[3 * kSlots + kNbhdSlot] > 0) {
-            wstride = (3 * ((tier_max[3] + 31) / 32) + 31) & ~31u;
+            wstride = (4 * ((tier_max[3] + 31) / 32) + 31) & ~31u;
             const size_t words = (size_t)ctx->num_sms * kLargeDfsBlocksPerSm * 8 * wstride;
             BEEP_TRY(lp->alloc(wsc, words));
             LaunchRec ms;
